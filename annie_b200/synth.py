@@ -1,0 +1,69 @@
+"""Seeded synthetic inputs: xoshiro256** (Blackman & Vigna) seeded by splitmix64.
+
+Random odd b-bit N: b bits drawn little-endian from the generator, then the
+top bit and bit 0 are set.  Proth numbers k*2^n + 1 use k odd drawn from the
+same generator.
+"""
+
+MASK64 = (1 << 64) - 1
+
+
+def splitmix64(state):
+    state = (state + 0x9E3779B97F4A7C15) & MASK64
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+    return state, z ^ (z >> 31)
+
+
+def _rotl(x, k):
+    return ((x << k) | (x >> (64 - k))) & MASK64
+
+
+class Xoshiro256ss:
+    def __init__(self, seed):
+        st = seed & MASK64
+        self.s = []
+        for _ in range(4):
+            st, z = splitmix64(st)
+            self.s.append(z)
+
+    def next(self):
+        s = self.s
+        result = (_rotl((s[1] * 5) & MASK64, 7) * 9) & MASK64
+        t = (s[1] << 17) & MASK64
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = _rotl(s[3], 45)
+        return result
+
+    def uniform(self, lo, hi):
+        """Uniform integer in [lo, hi) (rejection sampling on 64-bit draws)."""
+        span = hi - lo
+        lim = (1 << 64) - ((1 << 64) % span)
+        while True:
+            x = self.next()
+            if x < lim:
+                return lo + x % span
+
+    def random_odd(self, bits):
+        words = (bits + 63) // 64
+        x = 0
+        for i in range(words):
+            x |= self.next() << (64 * i)
+        x &= (1 << bits) - 1
+        return x | (1 << (bits - 1)) | 1
+
+    def random(self):
+        return (self.next() >> 11) * (1.0 / (1 << 53))
+
+
+def random_odd(bits, seed):
+    return Xoshiro256ss(seed).random_odd(bits)
+
+
+def proth(k, n):
+    return k * (1 << n) + 1
