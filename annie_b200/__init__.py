@@ -1,0 +1,243 @@
+"""annie_b200: B200-native modular-squaring engine (PRP tests of large integers).
+
+Python mirror of the reference's ``transform`` interface (galloty/annie,
+src/transform.h:18-45) over the C ABI in include/annie_b200.h.  Integers are
+Python ints; registers are ``Transform.Reg0/Reg1/Reg2``.  The CUDA library is
+required: importing works without it, but creating a transform raises
+``EngineUnavailable`` when libannie_b200.so is missing or no CUDA device is
+present -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libannie_b200.so")
+
+AB_OK = 0
+AB_E_ARG = -1
+AB_E_UNSUPPORTED = -2
+AB_E_CUDA = -3
+AB_E_INIT_FAILED = -4
+AB_E_CHECKPOINT = -5
+AB_E_CAPACITY = -6
+AB_E_TIMEOUT = -7
+
+
+class EngineUnavailable(RuntimeError):
+    pass
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("annie_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [("K", C.c_int), ("pck", C.c_int), ("ln", C.c_int), ("lbase", C.c_int)]
+
+    def astuple(self):
+        return (self.K, self.pck, self.ln, self.lbase)
+
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_lib = None
+
+# (name, argtypes, restype) of every exported symbol of include/annie_b200.h
+ABI = [
+    ("ab_probe", [_u64p, C.c_size_t, C.c_int32, C.POINTER(Params), C.POINTER(Params), C.POINTER(C.c_int)], C.c_int),
+    ("ab_create", [_u64p, C.c_size_t, C.c_int32, C.c_int, C.POINTER(Params), C.POINTER(C.c_void_p)], C.c_int),
+    ("ab_destroy", [C.c_void_p], None),
+    ("ab_init_failed", [C.c_void_p], C.c_int),
+    ("ab_get_factor", [C.c_void_p, _u64p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    ("ab_info", [C.c_void_p, C.POINTER(Params)], C.c_int),
+    ("ab_set1", [C.c_void_p], C.c_int),
+    ("ab_copy", [C.c_void_p, C.c_size_t, C.c_size_t], C.c_int),
+    ("ab_square_mul", [C.c_void_p, C.c_int32], C.c_int),
+    ("ab_mul", [C.c_void_p, C.c_size_t, C.c_size_t], C.c_int),
+    ("ab_get", [C.c_void_p, C.c_size_t, _u64p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    ("ab_checkpoint_size", [C.c_void_p], C.c_size_t),
+    ("ab_save_checkpoint", [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    ("ab_read_checkpoint", [C.c_void_p, C.c_void_p, C.c_size_t], C.c_int),
+    ("ab_read_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
+    ("ab_write_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
+    ("ab_synchronize", [C.c_void_p], C.c_int),
+    ("ab_square_mul_bits", [C.c_void_p, _u64p, C.c_size_t, C.c_int32], C.c_int),
+    ("ab_timer_start", [C.c_void_p], C.c_int),
+    ("ab_timer_stop", [C.c_void_p, C.POINTER(C.c_float)], C.c_int),
+    ("ab_last_error", [], C.c_char_p),
+    ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
+    ("ab_diag_product", [C.c_void_p, C.c_int, _u32p, _u32p, C.c_uint32, _u32p, C.c_int, _u32p], C.c_int),
+]
+
+
+def lib(build_if_missing=False):
+    """The loaded C ABI library (built in-tree by annie_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            if build_if_missing:
+                from . import build
+                build.build()
+            else:
+                raise EngineUnavailable("CUDA engine not built: %s missing (run python -m annie_b200.build)" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, args, res in ABI:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != AB_OK:
+        raise EngineError(rc, lib().ab_last_error().decode(errors="replace"))
+
+
+def int_to_limbs(x):
+    n = max(1, (x.bit_length() + 63) // 64)
+    return np.frombuffer(x.to_bytes(n * 8, "little"), dtype=np.uint64).copy()
+
+
+def limbs_to_int(a, count):
+    return int.from_bytes(np.asarray(a[:count], dtype=np.uint64).tobytes(), "little")
+
+
+def probe(N, a, forced=None):
+    """(params tuple, init_failed) by the factory rule of transformGPU.h:822-857; no GPU needed."""
+    limbs = int_to_limbs(N)
+    out = Params()
+    failed = C.c_int()
+    fp = None if forced is None else C.byref(Params(*forced))
+    _check(lib().ab_probe(limbs.ctypes.data_as(_u64p), len(limbs), a, fp, C.byref(out), C.byref(failed)))
+    return out.astuple(), bool(failed.value)
+
+
+class Transform:
+    """The reference's transform register machine on one GPU (transform.h:18-45)."""
+
+    Reg0, Reg1, Reg2 = 0, 1, 2
+
+    def __init__(self, N, a, device=0, params=None):
+        self.N, self.a = N, a
+        L = lib()
+        limbs = int_to_limbs(N)
+        h = C.c_void_p()
+        fp = None if params is None else C.byref(Params(*params))
+        _check(L.ab_create(limbs.ctypes.data_as(_u64p), len(limbs), a, device, fp, C.byref(h)))
+        self.h = h
+        self.L = L
+        info = Params()
+        _check(L.ab_info(h, C.byref(info)))
+        self.K, self.pck, self.ln, self.lbase = info.astuple()
+        self.n = 1 << self.ln
+        self._cap = len(limbs) + 2
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ab_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- transform.h:26-34
+    def init_failed(self):
+        return bool(self.L.ab_init_failed(self.h))
+
+    def get_factor(self):
+        out = np.zeros(self._cap, dtype=np.uint64)
+        cnt = C.c_size_t()
+        _check(self.L.ab_get_factor(self.h, out.ctypes.data_as(_u64p), len(out), C.byref(cnt)))
+        return limbs_to_int(out, cnt.value)
+
+    def set1(self):
+        _check(self.L.ab_set1(self.h))
+
+    def copy(self, dst, src):
+        _check(self.L.ab_copy(self.h, dst, src))
+
+    def square_mul(self, a):
+        _check(self.L.ab_square_mul(self.h, a))
+
+    def square_mul_bits(self, bits, count, a):
+        """count squarings; step i multiplies by a when bit i of `bits` (an int) is set."""
+        words = np.frombuffer(bits.to_bytes(max(8, (count + 63) // 64 * 8), "little"), dtype=np.uint64).copy()
+        _check(self.L.ab_square_mul_bits(self.h, words.ctypes.data_as(_u64p), count, a))
+
+    def mul(self, dst, src):
+        _check(self.L.ab_mul(self.h, dst, src))
+
+    def get(self, src):
+        out = np.zeros(self._cap, dtype=np.uint64)
+        cnt = C.c_size_t()
+        _check(self.L.ab_get(self.h, src, out.ctypes.data_as(_u64p), len(out), C.byref(cnt)))
+        return limbs_to_int(out, cnt.value)
+
+    # -- checkpoint payload (transformGPU.h:608-641)
+    def save_checkpoint(self):
+        size = self.L.ab_checkpoint_size(self.h)
+        buf = np.zeros(size, dtype=np.uint8)
+        written = C.c_size_t()
+        _check(self.L.ab_save_checkpoint(self.h, buf.ctypes.data_as(C.c_void_p), size, C.byref(written)))
+        return buf.tobytes()
+
+    def read_checkpoint(self, payload):
+        buf = np.frombuffer(payload, dtype=np.uint8).copy()
+        rc = self.L.ab_read_checkpoint(self.h, buf.ctypes.data_as(C.c_void_p), len(buf))
+        if rc == AB_E_CHECKPOINT:
+            return False
+        _check(rc)
+        return True
+
+    def read_register(self, reg):
+        out = np.zeros(self.K * self.n, dtype=np.uint32)
+        _check(self.L.ab_read_register(self.h, reg, out.ctypes.data_as(_u32p), len(out)))
+        return out
+
+    def write_register(self, reg, words):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        _check(self.L.ab_write_register(self.h, reg, w.ctypes.data_as(_u32p), len(w)))
+
+    def synchronize(self):
+        _check(self.L.ab_synchronize(self.h))
+
+    def timer_start(self):
+        _check(self.L.ab_timer_start(self.h))
+
+    def timer_stop(self):
+        ms = C.c_float()
+        _check(self.L.ab_timer_stop(self.h, C.byref(ms)))
+        return ms.value
+
+    # -- information strings (transformGPU.h:766-795)
+    def get_info_short(self):
+        return "%d-prime NTT of length %d, packed-base = 2^{%dx%d}" % (self.K, self.n, self.pck, self.lbase)
+
+    def get_info(self):
+        return "Montgomery-McLaughlin-Gallot-Woltman reduction, " + self.get_info_short()
+
+    # -- diagnostics
+    def diag_forward(self, words, domain_q):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        out = np.zeros_like(w)
+        _check(self.L.ab_diag_forward(self.h, int(domain_q), w.ctypes.data_as(_u32p), out.ctypes.data_as(_u32p)))
+        return out
+
+    def diag_product(self, words, domain_q, a, xp=None, sub=None, lower_mode=0):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        out = np.zeros_like(w)
+        xpa = None if xp is None else np.ascontiguousarray(xp, dtype=np.uint32)
+        sba = None if sub is None else np.ascontiguousarray(sub, dtype=np.uint32)
+        _check(self.L.ab_diag_product(self.h, int(domain_q), w.ctypes.data_as(_u32p),
+                                      None if xpa is None else xpa.ctypes.data_as(_u32p), a,
+                                      None if sba is None else sba.ctypes.data_as(_u32p), lower_mode,
+                                      out.ctypes.data_as(_u32p)))
+        return out

@@ -1,0 +1,672 @@
+// Host engine of the modular-squaring transform and its C ABI
+// (include/annie_b200.h).
+//
+// The engine owns all device memory of one transform, drives the two NTT
+// passes of kernels.cu in the Montgomery-McLaughlin-Gallot-Woltman (MMGW)
+// sequence of the reference (src/transformGPU.h:523-568) and converts
+// integers to and from the RNS register layout on the host
+// (src/transformGPU.h:323-445).
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include <cuda_runtime.h>
+
+#include "gmp.h"
+#include "kernels.h"
+#include "../../include/annie_b200.h"
+
+using namespace ab;
+
+namespace
+{
+thread_local std::string g_last_error;
+
+struct ab_error : std::runtime_error
+{
+	int code;
+	ab_error(int c, const std::string & m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call) do { const cudaError_t e_ = (call); if (e_ != cudaSuccess) throw ab_error(AB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
+
+// ------------------------------------------------------------ host Z/pZ
+// The 14 primes of the reference and their primitive roots
+// (src/transformGPU.h:79-89).
+const u32 PRIMES[14] = {
+	(125u << 25) + 1, (243u << 24) + 1, (235u << 24) + 1, (29u << 27) + 1,
+	(13u << 28) + 1, (193u << 24) + 1, (3u << 30) + 1, (43u << 26) + 1,
+	(171u << 24) + 1, (81u << 25) + 1, (157u << 24) + 1, (151u << 24) + 1,
+	(37u << 26) + 1, (17u << 27) + 1 };
+const u32 PRIMROOTS[14] = { 3, 7, 3, 3, 3, 3, 5, 3, 35, 5, 3, 3, 3, 3 };
+
+struct HostZp
+{
+	u32 p, q, one, rsq;
+	explicit HostZp(u32 pp) : p(pp)
+	{
+		q = 1; for (int i = 0; i < 6; ++i) q *= 2 - p * q;      // p^-1 mod 2^32 (Newton)
+		one = (u32)(((u64)1 << 32) % p);
+		rsq = (u32)(((u64)one * one) % p);
+	}
+	u32 add(u32 a, u32 b) const { return a + b - ((a >= p - b) ? p : 0); }
+	u32 sub(u32 a, u32 b) const { return a - b + ((a < b) ? p : 0); }
+	u32 mul(u32 a, u32 b) const
+	{
+		const u64 t = (u64)a * b; const u32 m = (u32)t * q;
+		return sub((u32)(t >> 32), (u32)(((u64)m * p) >> 32));
+	}
+	u32 to_mont(u32 a) const { return mul(a % p, rsq); }
+	u32 pow(u32 x, u32 e) const { u32 r = one; while (e) { if (e & 1) r = mul(r, x); x = mul(x, x); e >>= 1; } return r; }
+	u32 inv(u32 x) const { return pow(x, p - 2); }
+};
+
+size_t bitrev(size_t i, size_t n)
+{
+	size_t r = 0;
+	for (size_t k = n, j = i; k > 1; k /= 2, j /= 2) r = (2 * r) | (j % 2);
+	return r;
+}
+
+// Twiddles w[S + bitrev(j, S)], S = n/4 .. 1, inverse at +n/2; w[0] is the
+// Montgomery form of w[1].  Domain R (x^n - 1) uses roots of unity of order
+// 2S, domain Q (x^n + 1) the twisted roots of order 4S (transformGPU.h:117-160).
+void make_roots(u32 * w, int ln, int k, bool domain_q)
+{
+	const HostZp z(PRIMES[k]);
+	const size_t n = (size_t)1 << ln;
+	u32 * wi = w + n / 2;
+	auto primroot_n = [&](int l) { return z.pow(z.to_mont(PRIMROOTS[k]), (z.p - 1) >> l); };
+	if (!domain_q)
+	{
+		u32 sr = primroot_n(ln - 1), sri = z.inv(sr);
+		for (size_t s = n / 4; s >= 1; s /= 2)
+		{
+			u32 t = z.one, ti = z.one;
+			for (size_t j = 0; j < s; ++j) { const size_t jr = bitrev(j, s); w[s + jr] = t; wi[s + jr] = ti; t = z.mul(t, sr); ti = z.mul(ti, sri); }
+			sr = z.mul(sr, sr); sri = z.mul(sri, sri);
+		}
+	}
+	else
+	{
+		u32 sr2 = primroot_n(ln), sr2i = z.inv(sr2);
+		for (size_t s = n / 4; s >= 1; s /= 2)
+		{
+			const u32 sr = z.mul(sr2, sr2), sri = z.mul(sr2i, sr2i);
+			u32 t = sr2, ti = sr2i;
+			for (size_t j = 0; j < s; ++j) { const size_t jr = bitrev(j, s); w[s + jr] = t; wi[s + jr] = ti; t = z.mul(t, sr); ti = z.mul(ti, sri); }
+			sr2 = sr; sr2i = sri;
+		}
+	}
+	w[0] = z.to_mont(w[1]);
+	wi[0] = 0;
+}
+
+size_t get_s(size_t K) { int s = -1; for (size_t k = K - 1; k != 0; k /= 2) ++s; return (size_t)1 << s; }
+
+// Parameter rule of the reference factory (transformGPU.h:798-850): for
+// K = 2..5 primes with packing get_s(K), the largest digit size that keeps
+// ln + 2 pck lbase < log2(prod P / 2a); keep the K with the smallest K n ln.
+void get_n_base(int & rln, int & rlbase, int pck, double log2_16aN, double log2_p_2a)
+{
+	for (int lbase = 31; lbase >= 2; --lbase)
+	{
+		int ln = 4; while (double(lbase * pck) * (1 << ln) < log2_16aN) ++ln;
+		const int log2_base = lbase * pck;
+		if (ln + 2 * log2_base < log2_p_2a) { rln = ln; rlbase = lbase; break; }
+	}
+}
+
+ab_params select_params(const mpz_t N, int32_t a)
+{
+	long e_n; const double m_n = mpz_get_d_2exp(&e_n, N);
+	const double log2_16aN = std::log2(16.0 * a) + std::log2(m_n) + e_n;
+	double l = std::log2(double(PRIMES[0])) - std::log2(2.0 * a);
+	uint64_t c_min = uint64_t(-1); size_t K_min = 0;
+	for (size_t K = 2; K < 6; ++K)
+	{
+		l += std::log2(double(PRIMES[K - 1]));
+		int ln = 0, lbase = 0; get_n_base(ln, lbase, (int)get_s(K), log2_16aN, l);
+		const uint64_t c = K * uint64_t(1u << ln) * uint64_t(ln);
+		if (c < c_min) { c_min = c; K_min = K; }
+	}
+	l = std::log2(double(PRIMES[0])) - std::log2(2.0 * a);
+	for (size_t k = 1; k < K_min; ++k) l += std::log2(double(PRIMES[k]));
+	ab_params p; p.K = (int)K_min; p.pck = (int)get_s(K_min); p.ln = 0; p.lbase = 0;
+	get_n_base(p.ln, p.lbase, p.pck, log2_16aN, l);
+	return p;
+}
+
+void mpz_from_limbs(mpz_t z, const uint64_t * limbs, size_t n) { mpz_import(z, n, -1, 8, 0, 0, limbs); }
+
+// 0: ok, else R = base^(pck n) - 1 shares a factor with N (stored in factor)
+bool compute_R_Ninv(const mpz_t N, const ab_params & p, mpz_t R, mpz_t Ninv, mpz_t factor)
+{
+	mpz_set_ui(R, 1);
+	mpz_mul_2exp(R, R, (mp_bitcnt_t)p.pck * (mp_bitcnt_t)p.lbase << p.ln);
+	mpz_sub_ui(R, R, 1);
+	if (mpz_invert(Ninv, N, R) == 0) { mpz_gcd(factor, N, R); return false; }
+	return true;
+}
+} // namespace
+
+// ============================================================ the engine
+struct ab_transform
+{
+	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, NQ, NIR, OPQ, OPR, AQ0, AQ1, AR0, AR1, TMP, WR, WQ, NBUF };
+
+	int device = 0;
+	cudaStream_t st = nullptr;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	ab_params prm{};
+	size_t n = 0;
+	Geometry geo{};
+	TConst tc{};
+	bool failed = false;
+	mpz_t N, factor;
+	u32 * dmem = nullptr;
+	bool prefwd = false;     // AQ0/AR0 hold the first forward levels of REG0
+	std::vector<u32> host;
+
+	u32 * b(int i) const { return dmem + (size_t)i * prm.K * n; }
+
+	~ab_transform()
+	{
+		if (dmem) cudaFree(dmem);
+		if (ev0) cudaEventDestroy(ev0);
+		if (ev1) cudaEventDestroy(ev1);
+		if (st) cudaStreamDestroy(st);
+		mpz_clears(N, factor, nullptr);
+	}
+
+	void build_consts()
+	{
+		const int K = prm.K;
+		std::memset(&tc, 0, sizeof(tc));
+		tc.K = K; tc.pck = prm.pck; tc.lbase = prm.lbase; tc.ln = prm.ln;
+		tc.n = (u32)n; tc.R = geo.R; tc.H = geo.H; tc.LA = geo.LA; tc.LB = geo.LB;
+		for (int k = 0; k < K; ++k)
+		{
+			const HostZp z(PRIMES[k]);
+			tc.p[k] = z.p; tc.q[k] = z.q; tc.rsq[k] = z.rsq;
+			tc.norm[k] = z.p - ((z.p - 1) >> (prm.ln - 1));
+			const u32 base = (u32)((1ull << prm.lbase) % z.p);
+			tc.rbase[k] = z.to_mont(base);
+			u32 bp = 1; for (int l = 0; l < prm.pck; ++l) bp = (u32)(((u64)bp * base) % z.p);
+			tc.rbase_pck[k] = bp;
+			const u32 b2 = (u32)(((u64)base * base) % z.p);
+			tc.b2m[k] = z.to_mont(b2); tc.b2mq[k] = tc.b2m[k] * z.q;
+			for (int j = k + 1; j < K; ++j)
+			{
+				tc.gm[k][j] = z.inv(z.to_mont(PRIMES[j] % z.p));   // Montgomery form of P_j^-1
+				tc.gmq[k][j] = tc.gm[k][j] * z.q;
+			}
+		}
+	}
+
+	// integer -> RNS register words (transformGPU.h:323-360)
+	void encode(const mpz_t x, u32 * out) const
+	{
+		const size_t nl = mpz_size(x);
+		const u64 * xl = (const u64 *)mpz_limbs_read(x);
+		const int lb = prm.lbase;
+		auto read_bits = [&](size_t bit) -> u32 {
+			const size_t li = bit / 64; const int sh = (int)(bit % 64);
+			const u64 lo = (li < nl) ? xl[li] : 0, hi = (li + 1 < nl) ? xl[li + 1] : 0;
+			u64 r = lo >> sh; if (sh != 0) r |= hi << (64 - sh);
+			return (u32)r & ((1u << lb) - 1);
+		};
+		size_t bit = 0;
+		for (size_t i = 0; i < n; ++i)
+		{
+			unsigned __int128 d = 0;
+			u32 dg[4];
+			for (int l = 0; l < prm.pck; ++l) { dg[l] = read_bits(bit); bit += (size_t)lb; }
+			for (int l = prm.pck - 1; l >= 0; --l) d = (d << lb) | dg[l];
+			for (int k = 0; k < prm.K; ++k) out[(size_t)k * n + i] = (u32)(d % PRIMES[k]);
+		}
+	}
+
+	// register words (first pck planes) -> integer y, then y mod N
+	// (transformGPU.h:362-445: CRT over the first pck primes, carry, pack)
+	void decode(const u32 * planes, mpz_t y) const
+	{
+		const int pck = prm.pck, lb = prm.lbase;
+		const size_t nbits = (size_t)pck * lb * n, nlimbs = nbits / 64 + 2;
+		std::vector<u64> out(nlimbs, 0);
+		HostZp z[4] = { HostZp(PRIMES[0]), HostZp(PRIMES[1 % 14]), HostZp(PRIMES[2]), HostZp(PRIMES[3]) };
+		u32 inv[4][4] = {};
+		for (int i = 0; i < pck; ++i)
+			for (int j = i + 1; j < pck; ++j) inv[i][j] = z[i].mul(z[i].inv(z[i].to_mont(PRIMES[j] % z[i].p)), 1);
+		__int128 f = 0; size_t bit = 0;
+		for (size_t i = 0; i < n; ++i)
+		{
+			u32 u[4];
+			for (int ii = pck - 1; ii >= 0; --ii)
+			{
+				u32 v = planes[(size_t)ii * n + i];
+				for (int j = pck - 1; j > ii; --j) v = (u32)(((u64)z[ii].sub(v, u[j]) * inv[ii][j]) % z[ii].p);
+				u[ii] = v;
+			}
+			const int32_t i0 = (u[0] > z[0].p / 2) ? (int32_t)(u[0] - z[0].p) : (int32_t)u[0];
+			__int128 D = i0;
+			for (int ii = 1; ii < pck; ++ii) D = D * z[ii].p + u[ii];
+			f += D;
+			for (int l = 0; l < pck; ++l)
+			{
+				const u64 r = (u64)(f & (((__int128)1 << lb) - 1));
+				const size_t li = bit / 64; const int sh = (int)(bit % 64);
+				out[li] |= r << sh; if (sh != 0 && sh + lb > 64) out[li + 1] |= r >> (64 - sh);
+				f >>= lb; bit += (size_t)lb;
+			}
+		}
+		mpz_import(y, nlimbs, -1, 8, 0, 0, out.data());
+		if (f != 0)
+		{
+			mpz_t F; mpz_init(F);
+			mpz_set_si(F, (long)f);
+			mpz_mul_2exp(F, F, (mp_bitcnt_t)nbits);
+			mpz_add(y, y, F);
+			mpz_clear(F);
+		}
+		mpz_mod(y, y, N);
+	}
+
+	// ---------------------------------------------------------- pass helpers
+	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
+	{
+		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st));
+	}
+	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
+	{
+		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st));
+	}
+	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp = nullptr) const
+	{
+		RowJob j; j.x = x; j.xp = xp; j.w = w; j.mode = mode; return j;
+	}
+	ColJob cj_norm(const u32 * in) const
+	{
+		ColJob j; std::memset(&j, 0, sizeof(j)); j.in = in; j.transformed = 0; j.a = 1; return j;
+	}
+	ColJob cj_tr(const u32 * in, const u32 * w_in, u32 a, int nega, const u32 * sub, int lower) const
+	{
+		ColJob j; std::memset(&j, 0, sizeof(j));
+		j.in = in; j.transformed = 1; j.w_in = w_in; j.a = a; j.nega = nega; j.sub = sub; j.lower = lower;
+		return j;
+	}
+	static void set_fwd(ColJob & j, u32 * q_out, const u32 * wq, u32 * r_out, const u32 * wr)
+	{
+		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wq : nullptr;
+		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wr : nullptr;
+	}
+
+	// full forward transform of a normal-form register in one or two domains
+	void full_forward(const u32 * src, u32 * dq, u32 * dr)
+	{
+		ColJob j = cj_norm(src); set_fwd(j, dq, b(WQ), dr, b(WR)); cols(j);
+		if (dq && dr) { RowJob a = rj(dq, ROW_FWD_ONLY, b(WQ)), c = rj(dr, ROW_FWD_ONLY, b(WR)); rows(a, &c); }
+		else if (dq) rows(rj(dq, ROW_FWD_ONLY, b(WQ)));
+		else rows(rj(dr, ROW_FWD_ONLY, b(WR)));
+	}
+
+	// reduceMMGW tail (transformGPU.h:523-538): m' = T_R Ninv mod R, +2,
+	// r' = m' N - T_Q mod Q.  AR1 holds the first forward levels of T_R.
+	void reduce_tail(const u32 * tq, u32 * out, bool want_prefwd)
+	{
+		rows(rj(b(AR1), ROW_MUL, b(WR), b(NIR)));
+		ColJob j1 = cj_tr(b(AR1), b(WR), 1, 0, nullptr, LOWER_R_ADD2); set_fwd(j1, b(AQ1), b(WQ), nullptr, nullptr); cols(j1);
+		rows(rj(b(AQ1), ROW_MUL, b(WQ), b(NQ)));
+		ColJob j2 = cj_tr(b(AQ1), b(WQ), 1, 1, tq, LOWER_Q); j2.out_norm = out;
+		if (want_prefwd) set_fwd(j2, b(AQ0), b(WQ), b(AR0), b(WR));
+		cols(j2);
+	}
+
+	// squareMMGW (transformGPU.h:556-568)
+	void square_mul(u32 a)
+	{
+		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		RowJob rq = rj(b(AQ0), ROW_SQUARE, b(WQ)), rr = rj(b(AR0), ROW_SQUARE, b(WR));
+		rows(rq, &rr);
+		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
+		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
+		cols(jq, &jr);
+		reduce_tail(b(TQ), b(REG0), true);
+		prefwd = true;
+	}
+
+	// mulMMGW (transformGPU.h:540-554)
+	void mul(int dst, int src)
+	{
+		full_forward(b(src), b(OPQ), b(OPR));
+		{ ColJob j = cj_norm(b(dst)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		prefwd = false;
+		RowJob rq = rj(b(AQ0), ROW_MUL, b(WQ), b(OPQ)), rr = rj(b(AR0), ROW_MUL, b(WR), b(OPR));
+		rows(rq, &rr);
+		ColJob jq = cj_tr(b(AQ0), b(WQ), 1, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
+		ColJob jr = cj_tr(b(AR0), b(WR), 1, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
+		cols(jq, &jr);
+		reduce_tail(b(TQ), b(dst), dst == REG0);
+		prefwd = (dst == REG0);
+	}
+
+	// conversion out of MMGW form into TMP (transformGPU.h:576-586)
+	void reduce_copy(int src)
+	{
+		ColJob j = cj_norm(b(src)); set_fwd(j, nullptr, nullptr, b(AR1), b(WR)); cols(j);
+		reduce_tail(b(src), b(TMP), false);
+	}
+
+	void copy(int dst, int src)
+	{
+		if (dst == src) return;
+		CK(cudaMemcpyAsync(b(dst), b(src), (size_t)prm.K * n * 4, cudaMemcpyDeviceToDevice, st));
+		if (dst == REG0) prefwd = false;
+	}
+
+	void upload(int buf, const u32 * src)
+	{
+		CK(cudaMemcpyAsync(b(buf), src, (size_t)prm.K * n * 4, cudaMemcpyHostToDevice, st));
+		CK(cudaStreamSynchronize(st));
+	}
+	void download(int buf, u32 * dst, size_t planes)
+	{
+		CK(cudaMemcpyAsync(dst, b(buf), planes * n * 4, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+	}
+
+	void get(int src, mpz_t z)
+	{
+		reduce_copy(src);
+		host.resize((size_t)prm.K * n);
+		download(TMP, host.data(), (size_t)prm.pck);
+		decode(host.data(), z);
+	}
+
+	void init(const mpz_t Nin, int32_t a, int dev, const ab_params * forced)
+	{
+		mpz_inits(N, factor, nullptr);
+		mpz_set(N, Nin);
+		device = dev;
+		prm = forced ? *forced : select_params(N, a);
+		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31)
+			throw ab_error(AB_E_ARG, "invalid transform parameters");
+		if (!make_geometry(prm.ln, 0, geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length 2^" + std::to_string(prm.ln) + " is not supported (6 <= ln <= 20)");
+		n = (size_t)1 << prm.ln;
+		mpz_t R, Ninv; mpz_inits(R, Ninv, nullptr);
+		if (!compute_R_Ninv(N, prm, R, Ninv, factor)) { failed = true; mpz_clears(R, Ninv, nullptr); return; }
+		build_consts();
+
+		CK(cudaSetDevice(device));
+		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
+		CK(cudaMalloc(&dmem, (size_t)NBUF * prm.K * n * 4));
+		CK(cudaMemsetAsync(dmem, 0, (size_t)NBUF * prm.K * n * 4, st));
+
+		host.assign((size_t)prm.K * n, 0);
+		std::vector<u32> wr((size_t)prm.K * n), wq((size_t)prm.K * n);
+		for (int k = 0; k < prm.K; ++k) { make_roots(&wr[(size_t)k * n], prm.ln, k, false); make_roots(&wq[(size_t)k * n], prm.ln, k, true); }
+		upload(WR, wr.data()); upload(WQ, wq.data());
+
+		encode(N, host.data()); upload(TMP, host.data());
+		full_forward(b(TMP), b(NQ), nullptr);
+		CK(cudaStreamSynchronize(st));
+		encode(Ninv, host.data()); upload(TMP, host.data());
+		full_forward(b(TMP), nullptr, b(NIR));
+		CK(cudaStreamSynchronize(st));
+		// MMGW form of 1 is R/2 mod N (transformGPU.h:743-747)
+		mpz_mod(Ninv, R, N);
+		if (mpz_odd_p(Ninv)) mpz_add(Ninv, Ninv, N);
+		mpz_fdiv_q_2exp(Ninv, Ninv, 1);
+		encode(Ninv, host.data()); upload(ONE, host.data());
+		mpz_clears(R, Ninv, nullptr);
+	}
+};
+
+// ============================================================ C ABI
+namespace
+{
+template <typename F>
+int guarded(F && f)
+{
+	try { f(); return AB_OK; }
+	catch (const ab_error & e) { g_last_error = e.what(); return e.code; }
+	catch (const std::exception & e) { g_last_error = e.what(); return AB_E_ARG; }
+}
+
+bool valid_reg(size_t r) { return r <= 2; }
+
+void need_ready(const ab_transform * h)
+{
+	if (h == nullptr) throw ab_error(AB_E_ARG, "null handle");
+	if (h->failed) throw ab_error(AB_E_INIT_FAILED, "gcd(N, R) != 1");
+}
+}
+
+extern "C" {
+
+int ab_probe(const uint64_t * Nl, size_t nlimbs, int32_t a, const ab_params * forced, ab_params * out, int * init_failed)
+{
+	return guarded([&] {
+		if (Nl == nullptr || nlimbs == 0 || out == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		mpz_t N, R, Ninv, f; mpz_inits(N, R, Ninv, f, nullptr);
+		mpz_from_limbs(N, Nl, nlimbs);
+		*out = forced ? *forced : select_params(N, a);
+		if (init_failed) *init_failed = compute_R_Ninv(N, *out, R, Ninv, f) ? 0 : 1;
+		mpz_clears(N, R, Ninv, f, nullptr);
+	});
+}
+
+int ab_create(const uint64_t * Nl, size_t nlimbs, int32_t a, int device, const ab_params * forced, ab_transform ** out)
+{
+	if (out) *out = nullptr;
+	ab_transform * h = nullptr;
+	const int rc = guarded([&] {
+		if (Nl == nullptr || nlimbs == 0 || out == nullptr || a < 1) throw ab_error(AB_E_ARG, "bad arguments");
+		mpz_t N; mpz_init(N); mpz_from_limbs(N, Nl, nlimbs);
+		h = new ab_transform();
+		try { h->init(N, a, device, forced); }
+		catch (...) { mpz_clear(N); throw; }
+		mpz_clear(N);
+	});
+	if (rc != AB_OK) { delete h; return rc; }
+	*out = h;
+	return AB_OK;
+}
+
+void ab_destroy(ab_transform * h) { delete h; }
+
+int ab_init_failed(const ab_transform * h) { return (h != nullptr && h->failed) ? 1 : 0; }
+
+int ab_get_factor(const ab_transform * h, uint64_t * out, size_t cap, size_t * count)
+{
+	return guarded([&] {
+		if (h == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		const mpz_srcptr z = h->failed ? h->factor : h->N;
+		const size_t sz = mpz_size(z);
+		if (sz > cap) throw ab_error(AB_E_CAPACITY, "output too small");
+		for (size_t i = 0; i < sz; ++i) out[i] = mpz_getlimbn(z, (mp_size_t)i);
+		*count = sz;
+	});
+}
+
+int ab_info(const ab_transform * h, ab_params * out)
+{
+	return guarded([&] { if (h == nullptr || out == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); *out = h->prm; });
+}
+
+int ab_set1(ab_transform * h)
+{
+	return guarded([&] { need_ready(h); h->copy(ab_transform::REG0, ab_transform::ONE); });
+}
+
+int ab_copy(ab_transform * h, size_t dst, size_t src)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(dst) || !valid_reg(src)) throw ab_error(AB_E_ARG, "register index");
+		h->copy((int)dst, (int)src);
+	});
+}
+
+int ab_square_mul(ab_transform * h, int32_t a)
+{
+	return guarded([&] { need_ready(h); h->square_mul((u32)a); });
+}
+
+int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, int32_t a)
+{
+	return guarded([&] {
+		need_ready(h);
+		for (size_t i = 0; i < count; ++i) h->square_mul(((bits[i / 64] >> (i % 64)) & 1) ? (u32)a : 1u);
+	});
+}
+
+int ab_mul(ab_transform * h, size_t dst, size_t src)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(dst) || !valid_reg(src)) throw ab_error(AB_E_ARG, "register index");
+		h->mul((int)dst, (int)src);
+	});
+}
+
+int ab_get(ab_transform * h, size_t src, uint64_t * out, size_t cap, size_t * count)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(src) || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		mpz_t z; mpz_init(z);
+		h->get((int)src, z);
+		const size_t sz = mpz_size(z);
+		if (sz > cap) { mpz_clear(z); throw ab_error(AB_E_CAPACITY, "output too small"); }
+		for (size_t i = 0; i < sz; ++i) out[i] = mpz_getlimbn(z, (mp_size_t)i);
+		*count = sz;
+		mpz_clear(z);
+	});
+}
+
+size_t ab_checkpoint_size(const ab_transform * h)
+{
+	return (h == nullptr) ? 0 : 8 + (size_t)8 * h->prm.K * h->n;
+}
+
+int ab_save_checkpoint(ab_transform * h, void * buf, size_t cap, size_t * written)
+{
+	return guarded([&] {
+		need_ready(h);
+		const size_t need = ab_checkpoint_size(h), K = (size_t)h->prm.K, n = h->n;
+		if (buf == nullptr || cap < need) throw ab_error(AB_E_CAPACITY, "checkpoint buffer too small");
+		std::vector<u32> r0(K * n), r1(K * n);
+		h->download(ab_transform::REG0, r0.data(), K);
+		h->download(ab_transform::REG1, r1.data(), K);
+		u32 * o = static_cast<u32 *>(buf);
+		o[0] = (u32)K; o[1] = (u32)n;
+		for (size_t k = 0; k < K; ++k)
+		{
+			std::memcpy(o + 2 + 2 * k * n, &r0[k * n], n * 4);
+			std::memcpy(o + 2 + 2 * k * n + n, &r1[k * n], n * 4);
+		}
+		if (written) *written = need;
+	});
+}
+
+int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size)
+{
+	return guarded([&] {
+		need_ready(h);
+		const size_t K = (size_t)h->prm.K, n = h->n;
+		if (buf == nullptr || size < 8) throw ab_error(AB_E_CHECKPOINT, "checkpoint too short");
+		const u32 * in = static_cast<const u32 *>(buf);
+		if (in[0] != K || in[1] != n || size < ab_checkpoint_size(h)) throw ab_error(AB_E_CHECKPOINT, "checkpoint does not match K or n");
+		std::vector<u32> r0(K * n), r1(K * n);
+		for (size_t k = 0; k < K; ++k)
+		{
+			std::memcpy(&r0[k * n], in + 2 + 2 * k * n, n * 4);
+			std::memcpy(&r1[k * n], in + 2 + 2 * k * n + n, n * 4);
+		}
+		h->upload(ab_transform::REG0, r0.data());
+		h->upload(ab_transform::REG1, r1.data());
+		h->prefwd = false;
+	});
+}
+
+int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_words)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(reg) || out == nullptr || cap_words < (size_t)h->prm.K * h->n) throw ab_error(AB_E_ARG, "bad arguments");
+		h->download((int)reg, out, (size_t)h->prm.K);
+	});
+}
+
+int ab_write_register(ab_transform * h, size_t reg, const uint32_t * in, size_t nwords)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(reg) || in == nullptr || nwords != (size_t)h->prm.K * h->n) throw ab_error(AB_E_ARG, "bad arguments");
+		h->upload((int)reg, in);
+		if (reg == 0) h->prefwd = false;
+	});
+}
+
+int ab_synchronize(ab_transform * h)
+{
+	return guarded([&] { if (h == nullptr) throw ab_error(AB_E_ARG, "null handle"); if (h->st) CK(cudaStreamSynchronize(h->st)); });
+}
+
+int ab_timer_start(ab_transform * h)
+{
+	return guarded([&] { need_ready(h); CK(cudaEventRecord(h->ev0, h->st)); });
+}
+
+int ab_timer_stop(ab_transform * h, float * ms)
+{
+	return guarded([&] {
+		need_ready(h);
+		CK(cudaEventRecord(h->ev1, h->st));
+		CK(cudaEventSynchronize(h->ev1));
+		CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+	});
+}
+
+const char * ab_last_error(void) { return g_last_error.c_str(); }
+
+int ab_diag_forward(ab_transform * h, int domain, const uint32_t * in, uint32_t * out)
+{
+	return guarded([&] {
+		need_ready(h);
+		h->upload(ab_transform::TMP, in);
+		if (domain) h->full_forward(h->b(ab_transform::TMP), h->b(ab_transform::AQ1), nullptr);
+		else h->full_forward(h->b(ab_transform::TMP), nullptr, h->b(ab_transform::AQ1));
+		h->download(ab_transform::AQ1, out, (size_t)h->prm.K);
+	});
+}
+
+int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * xp, uint32_t a,
+	const uint32_t * sub, int lower_mode, uint32_t * out)
+{
+	return guarded([&] {
+		need_ready(h);
+		using T = ab_transform;
+		const u32 * w = h->b(domain ? T::WQ : T::WR);
+		h->upload(T::TMP, in);
+		if (xp) h->upload(T::OPQ, xp);
+		if (sub) h->upload(T::OPR, sub);
+		ColJob j = h->cj_norm(h->b(T::TMP));
+		if (domain) T::set_fwd(j, h->b(T::AQ1), w, nullptr, nullptr); else T::set_fwd(j, nullptr, nullptr, h->b(T::AQ1), w);
+		h->cols(j);
+		h->rows(h->rj(h->b(T::AQ1), xp ? ROW_MUL : ROW_SQUARE, w, xp ? h->b(T::OPQ) : nullptr));
+		ColJob c = h->cj_tr(h->b(T::AQ1), w, a, domain ? 1 : 0, sub ? h->b(T::OPR) : nullptr, lower_mode);
+		c.out_norm = h->b(T::TMP);
+		h->cols(c);
+		h->download(T::TMP, out, (size_t)h->prm.K);
+		h->prefwd = false;
+	});
+}
+
+}

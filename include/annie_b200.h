@@ -1,0 +1,110 @@
+/*
+ * annie_b200: B200-native modular-squaring engine behind a C ABI.
+ *
+ * Drop-in for the reference's GPU transform (galloty/annie):
+ *   class transform            src/transform.h:18-45     (the register machine)
+ *   create_transformGPU(...)   src/transformGPU.h:822-885 (factory + parameter rule)
+ *   transformGPU<LN>           src/transformGPU.h:286-796 (the engine the C++ host drives)
+ * A C++ class implementing `transform` on top of these calls is in
+ * annie_b200/host/transformCUDA.h.
+ *
+ * Numbers cross the ABI as little-endian arrays of 64-bit limbs (the layout of
+ * GMP's mpz limbs on LP64).  Registers 0, 1, 2 are the reference's Reg0..Reg2.
+ * Every function returns AB_OK (0) or a negative status; ab_last_error()
+ * describes the last failure of the calling thread.  A handle is not
+ * re-entrant: one host thread at a time per handle (as the reference).
+ */
+#ifndef ANNIE_B200_H
+#define ANNIE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AB_OK              0
+#define AB_E_ARG          -1   /* bad argument (register index, size, null pointer) */
+#define AB_E_UNSUPPORTED  -2   /* NTT length outside the supported range */
+#define AB_E_CUDA         -3   /* CUDA runtime error */
+#define AB_E_INIT_FAILED  -4   /* gcd(N, R) != 1: see ab_get_factor (transformGPU.h:655-661) */
+#define AB_E_CHECKPOINT   -5   /* checkpoint payload does not match K or n (transformGPU.h:608-624) */
+#define AB_E_CAPACITY     -6   /* output buffer too small */
+#define AB_E_TIMEOUT      -7   /* a device wait ran past its iteration limit */
+
+typedef struct ab_transform ab_transform;
+
+/* Transform parameters: K primes, packing pck = digits per coefficient,
+   NTT length 2^ln, digit size 2^lbase (transformGPU.h:644-645). */
+typedef struct
+{
+	int K, pck, ln, lbase;
+} ab_params;
+
+/* Parameter rule of create_transformGPU (transformGPU.h:822-857), or the
+   forced parameters; init_failed = gcd(N, base^(pck n) - 1) != 1.  Host only. */
+int ab_probe(const uint64_t * N, size_t nlimbs, int32_t a, const ab_params * forced,
+	ab_params * out, int * init_failed);
+
+/* create_transformGPU(N, a, device) (transformGPU.h:822) + constructor
+   (transformGPU.h:644-753).  `forced` may be NULL.  If gcd(N, R) != 1 the
+   handle is still created, ab_init_failed() returns 1 and ab_get_factor()
+   gives the gcd (transformGPU.h:655-661, annie.h:269-283). */
+int ab_create(const uint64_t * N, size_t nlimbs, int32_t a, int device, const ab_params * forced,
+	ab_transform ** out);
+void ab_destroy(ab_transform * h);                                   /* ~transformGPU (transformGPU.h:755-764) */
+
+int ab_init_failed(const ab_transform * h);                          /* transform::init_failed (transform.h:32) */
+int ab_get_factor(const ab_transform * h, uint64_t * out, size_t cap, size_t * count); /* transform::get_factor (transform.h:33) */
+int ab_info(const ab_transform * h, ab_params * out);                /* transform::get_info_short (transformGPU.h:784-789) */
+
+int ab_set1(ab_transform * h);                                       /* transform::set1  (transform.h:26, transformGPU.h:571-574) */
+int ab_copy(ab_transform * h, size_t dst, size_t src);               /* transform::copy  (transform.h:28, transformGPU.h:588-591) */
+int ab_square_mul(ab_transform * h, int32_t a);                      /* transform::square_mul (transform.h:29, transformGPU.h:593-596) */
+int ab_mul(ab_transform * h, size_t dst, size_t src);                /* transform::mul   (transform.h:30, transformGPU.h:598-601) */
+/* transform::get (transform.h:27, transformGPU.h:576-586): r_src out of
+   MMGW form, reduced mod N; `count` = limbs written. */
+int ab_get(ab_transform * h, size_t src, uint64_t * out, size_t cap, size_t * count);
+
+/* transform::save_checkpoint / read_checkpoint (transform.h:37-38,
+   transformGPU.h:608-641): payload = u32 K, u32 n, then per prime k the words
+   of Reg0 and Reg1 (2n u32).  Size = 8 + 8 K n bytes. */
+size_t ab_checkpoint_size(const ab_transform * h);
+int ab_save_checkpoint(ab_transform * h, void * buf, size_t cap, size_t * written);
+int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size);
+
+/* Raw register words (K planes of n u32, normal form) -- the engine's
+   read_memory / write_memory (engine.h of the reference). */
+int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_words);
+int ab_write_register(ab_transform * h, size_t reg, const uint32_t * in, size_t nwords);
+
+/* Waits for all work queued on the handle's stream. */
+int ab_synchronize(ab_transform * h);
+
+/* Runs `count` square_mul steps whose multipliers are `a` where the bit of
+   `bits` (LSB first, bit i for step i) is set and 1 elsewhere -- the inner
+   loop of annie::check (annie.h:319-341) without the Gerbicz-Li product. */
+int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, int32_t a);
+
+/* Device time of the work queued since the last call, in milliseconds
+   (CUDA events on the handle's stream). */
+int ab_timer_start(ab_transform * h);
+int ab_timer_stop(ab_transform * h, float * ms);
+
+const char * ab_last_error(void);
+
+/* Diagnostics (kernel-level parity tests): run one stage on host data.
+   ab_diag_forward:  full forward NTT of a normal-form register (domain 0 = R, 1 = Q).
+   ab_diag_product:  forward NTT, pointwise square (xp == NULL) or product with the
+                     forward image xp, inverse NTT, carry (a, nega for domain Q,
+                     optional subtraction, lower_mode 0 none / 1 mod R + 2 / 2 mod Q). */
+int ab_diag_forward(ab_transform * h, int domain, const uint32_t * in, uint32_t * out);
+int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * xp,
+	uint32_t a, const uint32_t * sub, int lower_mode, uint32_t * out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,151 @@
+"""GPU parity: the CUDA engine against the oracle (C restatement of the
+reference transform), bit-exact, through the C ABI.
+
+Kernel level: full forward NTT; forward + pointwise square/multiply + inverse
++ carry (+ subtraction, + mod R/Q fix-up), for K = 2..5 primes.
+Register level: raw register words after every square_mul / mul equal the
+oracle's.  Integer level: get() equals pow(a, e, N).
+"""
+import numpy as np
+import pytest
+
+import annie_b200 as A
+from helpers import pick_N, random_digits_register, random_residues
+
+pytestmark = pytest.mark.gpu
+
+# (K, ln, lbase) -- pck follows from K (1, 2, 2, 4)
+KERNEL_CASES = [
+    (5, 6, 18), (5, 8, 18), (5, 10, 18), (5, 12, 18), (5, 13, 17), (5, 15, 17),
+    (4, 11, 28), (4, 16, 27), (3, 9, 22), (2, 10, 14), (5, 19, 17),
+]
+
+
+def _pck(K):
+    return {2: 1, 3: 2, 4: 2, 5: 4}[K]
+
+
+def _pair(oracle_mod, K, ln, lbase, seed=11):
+    params = (K, _pck(K), ln, lbase)
+    bits = max(64, (_pck(K) * lbase << ln) // 2)
+    N = None
+    from annie_b200.synth import Xoshiro256ss
+    rng = Xoshiro256ss(seed)
+    for _ in range(100):
+        cand = rng.random_odd(bits)
+        _, failed = A.probe(cand, 3, forced=params)
+        if not failed:
+            N = cand
+            break
+    assert N is not None
+    return A.Transform(N, 3, params=params), oracle_mod.Oracle(N, 3, params=params)
+
+
+@pytest.mark.parametrize("K,ln,lbase", KERNEL_CASES)
+def test_forward_ntt(oracle_mod, K, ln, lbase):
+    t, o = _pair(oracle_mod, K, ln, lbase)
+    x = random_residues(K, ln, seed=ln * 7 + K)
+    for dom in (0, 1):
+        got = t.diag_forward(x, dom)
+        exp = o.fwd_full(x, dom)
+        assert np.array_equal(got, exp), "forward NTT mismatch (domain %d): %d words differ" % (dom, np.count_nonzero(got != exp))
+
+
+@pytest.mark.parametrize("K,ln,lbase", KERNEL_CASES)
+def test_square_carry(oracle_mod, K, ln, lbase):
+    t, o = _pair(oracle_mod, K, ln, lbase)
+    pck = _pck(K)
+    x = random_digits_register(K, pck, ln, lbase, seed=ln + 100 * K)
+    for dom in (0, 1):
+        for a in (1, 3):
+            got = t.diag_product(x, dom, a)
+            y = o.inv_full(o.pointwise(o.fwd_full(x, dom), dom), dom)
+            exp = o.carry(y, a, nega=dom)
+            assert np.array_equal(got, exp), "square+carry mismatch dom=%d a=%d: %d words differ" % (dom, a, np.count_nonzero(got != exp))
+
+
+@pytest.mark.parametrize("K,ln,lbase", KERNEL_CASES)
+def test_mul_sub_lower(oracle_mod, K, ln, lbase):
+    t, o = _pair(oracle_mod, K, ln, lbase)
+    pck = _pck(K)
+    x = random_digits_register(K, pck, ln, lbase, seed=ln + 200 * K)
+    y = random_digits_register(K, pck, ln, lbase, seed=ln + 300 * K)
+    s = random_digits_register(K, pck, ln, lbase, seed=ln + 400 * K)
+    for dom, lower in ((0, 1), (1, 2), (1, 0)):
+        xp = o.fwd_full(y, dom)
+        got = t.diag_product(x, dom, 1, xp=xp, sub=(s if dom == 1 else None), lower_mode=lower)
+        z = o.inv_full(o.pointwise(o.fwd_full(x, dom), dom, xp), dom)
+        exp = o.carry(z, 1, nega=dom, y=(s if dom == 1 else None), lower_mode=lower)
+        assert np.array_equal(got, exp), "mul/sub/lower mismatch dom=%d lower=%d: %d words differ" % (dom, lower, np.count_nonzero(got != exp))
+
+
+REG_CASES = [(5, 10, 18), (5, 12, 18), (4, 13, 27), (3, 11, 21), (5, 15, 17)]
+
+
+@pytest.mark.parametrize("K,ln,lbase", REG_CASES)
+def test_register_words_after_each_step(oracle_mod, K, ln, lbase):
+    t, o = _pair(oracle_mod, K, ln, lbase, seed=5)
+    t.set1(); o.set1()
+    t.copy(1, 0); o.copy(1, 0)
+    for i in range(5):
+        a = 3 if i % 2 == 0 else 1
+        t.square_mul(a); o.square_mul(a)
+        assert np.array_equal(t.read_register(0), o.read_reg(0)), "Reg0 differs after square_mul %d" % i
+    t.mul(1, 0); o.mul(1, 0)
+    assert np.array_equal(t.read_register(1), o.read_reg(1)), "Reg1 differs after mul"
+    t.copy(2, 0); o.copy(2, 0)
+    t.mul(2, 1); o.mul(2, 1)
+    assert np.array_equal(t.read_register(2), o.read_reg(2))
+    t.square_mul(3); o.square_mul(3)
+    assert np.array_equal(t.read_register(0), o.read_reg(0))
+    for r in range(3):
+        assert t.get(r) == o.get(r)
+
+
+@pytest.mark.parametrize("bits", [20000, 70000, 262144])
+def test_get_matches_pow(bits):
+    N = pick_N(bits, seed=bits)
+    t = A.Transform(N, 3)
+    t.set1()
+    e = 0
+    pattern = [3, 1, 1, 3, 3, 1, 3, 1, 1, 1, 3, 3]
+    for a in pattern:
+        t.square_mul(a)
+        e = 2 * e + (a == 3)
+    assert t.get(0) == pow(3, e, N)
+    t.copy(1, 0)
+    t.mul(1, 0)
+    assert t.get(1) == pow(3, 2 * e, N)
+
+
+def test_init_failed_reports_factor():
+    # N divisible by 3 shares a factor with R = 2^(pck lbase n) - 1 (annie.h:269-283)
+    from annie_b200.synth import Xoshiro256ss
+    rng = Xoshiro256ss(9)
+    while True:
+        N = rng.random_odd(40000)
+        if N % 3 == 0:
+            break
+    t = A.Transform(N, 3)
+    assert t.init_failed()
+    f = t.get_factor()
+    assert f > 1 and N % f == 0
+
+
+def test_checkpoint_round_trip(oracle_mod):
+    N = pick_N(100000, seed=21)
+    t = A.Transform(N, 3)
+    t.set1(); t.copy(1, 0)
+    for a in (3, 1, 3):
+        t.square_mul(a)
+    t.mul(1, 0)
+    payload = t.save_checkpoint()
+    assert len(payload) == 8 + 8 * t.K * t.n
+    r0, r1 = t.get(0), t.get(1)
+    t2 = A.Transform(N, 3)
+    assert t2.read_checkpoint(payload)
+    assert t2.get(0) == r0 and t2.get(1) == r1
+    t.square_mul(3); t2.square_mul(3)
+    assert np.array_equal(t.read_register(0), t2.read_register(0))
+    # a payload of another size is refused (transformGPU.h:613-616)
+    assert not t2.read_checkpoint(payload[:4] + (12345).to_bytes(4, "little") + payload[8:])
