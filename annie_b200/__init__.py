@@ -62,6 +62,8 @@ ABI = [
     ("ab_checkpoint_size", [C.c_void_p], C.c_size_t),
     ("ab_save_checkpoint", [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
     ("ab_read_checkpoint", [C.c_void_p, C.c_void_p, C.c_size_t], C.c_int),
+    ("ab_host_alloc", [C.c_size_t], C.c_void_p),
+    ("ab_host_free", [C.c_void_p], None),
     ("ab_read_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
     ("ab_write_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
     ("ab_synchronize", [C.c_void_p], C.c_int),
@@ -69,6 +71,9 @@ ABI = [
     ("ab_timer_start", [C.c_void_p], C.c_int),
     ("ab_timer_stop", [C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     ("ab_last_error", [], C.c_char_p),
+    ("ab_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
+    ("ab_profile_square", [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    ("ab_flush_l2", [C.c_void_p, C.c_size_t], C.c_int),
     ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
     ("ab_diag_product", [C.c_void_p, C.c_int, _u32p, _u32p, C.c_uint32, _u32p, C.c_int, _u32p], C.c_int),
 ]
@@ -197,6 +202,25 @@ class Transform:
         _check(rc)
         return True
 
+    def pinned(self, nbytes):
+        """A page-locked host buffer (numpy uint8 view) and its pointer; free with free_pinned."""
+        ptr = self.L.ab_host_alloc(nbytes)
+        if not ptr:
+            raise EngineError(AB_E_CUDA, "cudaMallocHost failed")
+        arr = np.ctypeslib.as_array((C.c_uint8 * nbytes).from_address(ptr))
+        return arr, ptr
+
+    def free_pinned(self, ptr):
+        self.L.ab_host_free(ptr)
+
+    def save_checkpoint_into(self, ptr, cap):
+        written = C.c_size_t()
+        _check(self.L.ab_save_checkpoint(self.h, C.c_void_p(ptr), cap, C.byref(written)))
+        return written.value
+
+    def read_checkpoint_from(self, ptr, size):
+        _check(self.L.ab_read_checkpoint(self.h, C.c_void_p(ptr), size))
+
     def read_register(self, reg):
         out = np.zeros(self.K * self.n, dtype=np.uint32)
         _check(self.L.ab_read_register(self.h, reg, out.ctypes.data_as(_u32p), len(out)))
@@ -216,6 +240,20 @@ class Transform:
         ms = C.c_float()
         _check(self.L.ab_timer_stop(self.h, C.byref(ms)))
         return ms.value
+
+    def launch_count(self):
+        c = C.c_uint64()
+        _check(self.L.ab_launch_count(self.h, C.byref(c)))
+        return c.value
+
+    def profile_square(self, a, cap=16):
+        ms = (C.c_float * cap)()
+        cnt = C.c_int()
+        _check(self.L.ab_profile_square(self.h, a, ms, cap, C.byref(cnt)))
+        return [ms[i] for i in range(cnt.value)]
+
+    def flush_l2(self, nbytes=256 << 20):
+        _check(self.L.ab_flush_l2(self.h, nbytes))
 
     # -- information strings (transformGPU.h:766-795)
     def get_info_short(self):

@@ -59,7 +59,7 @@ def build(force=False, ptxas_verbose=False, jobs=None):
             sys.stdout.write(out)
     if failed:
         raise RuntimeError("nvcc failed")
-    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-L" + os.path.dirname(GMP_SO), "-l:" + os.path.basename(GMP_SO), "-lcudart"]
+    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-L" + os.path.dirname(GMP_SO), "-l:" + os.path.basename(GMP_SO), "-cudart=static"]
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)

@@ -169,11 +169,17 @@ struct ab_transform
 	u32 * dmem = nullptr;
 	bool prefwd = false;     // AQ0/AR0 hold the first forward levels of REG0
 	std::vector<u32> host;
+	uint64_t launches = 0;   // kernels launched by this handle
+	std::vector<cudaEvent_t> prof;   // non-empty: record an event before every launch
+	size_t prof_used = 0;
+	void * flush_buf = nullptr;
 
 	u32 * b(int i) const { return dmem + (size_t)i * prm.K * n; }
 
 	~ab_transform()
 	{
+		for (cudaEvent_t e : prof) cudaEventDestroy(e);
+		if (flush_buf) cudaFree(flush_buf);
 		if (dmem) cudaFree(dmem);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
@@ -275,15 +281,23 @@ struct ab_transform
 	}
 
 	// ---------------------------------------------------------- pass helpers
+	void mark()
+	{
+		if (prof_used < prof.size()) CK(cudaEventRecord(prof[prof_used++], st));
+	}
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		mark();
 		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st));
+		++launches;
 	}
 	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
 	{
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		mark();
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st));
+		++launches;
 	}
 	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp = nullptr) const
 	{
@@ -561,16 +575,15 @@ int ab_save_checkpoint(ab_transform * h, void * buf, size_t cap, size_t * writte
 		need_ready(h);
 		const size_t need = ab_checkpoint_size(h), K = (size_t)h->prm.K, n = h->n;
 		if (buf == nullptr || cap < need) throw ab_error(AB_E_CAPACITY, "checkpoint buffer too small");
-		std::vector<u32> r0(K * n), r1(K * n);
-		h->download(ab_transform::REG0, r0.data(), K);
-		h->download(ab_transform::REG1, r1.data(), K);
 		u32 * o = static_cast<u32 *>(buf);
 		o[0] = (u32)K; o[1] = (u32)n;
+		// per prime k: plane k of Reg0 then plane k of Reg1 (transformGPU.h:626-641)
 		for (size_t k = 0; k < K; ++k)
 		{
-			std::memcpy(o + 2 + 2 * k * n, &r0[k * n], n * 4);
-			std::memcpy(o + 2 + 2 * k * n + n, &r1[k * n], n * 4);
+			CK(cudaMemcpyAsync(o + 2 + 2 * k * n, h->b(ab_transform::REG0) + k * n, n * 4, cudaMemcpyDeviceToHost, h->st));
+			CK(cudaMemcpyAsync(o + 2 + 2 * k * n + n, h->b(ab_transform::REG1) + k * n, n * 4, cudaMemcpyDeviceToHost, h->st));
 		}
+		CK(cudaStreamSynchronize(h->st));
 		if (written) *written = need;
 	});
 }
@@ -583,17 +596,24 @@ int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size)
 		if (buf == nullptr || size < 8) throw ab_error(AB_E_CHECKPOINT, "checkpoint too short");
 		const u32 * in = static_cast<const u32 *>(buf);
 		if (in[0] != K || in[1] != n || size < ab_checkpoint_size(h)) throw ab_error(AB_E_CHECKPOINT, "checkpoint does not match K or n");
-		std::vector<u32> r0(K * n), r1(K * n);
 		for (size_t k = 0; k < K; ++k)
 		{
-			std::memcpy(&r0[k * n], in + 2 + 2 * k * n, n * 4);
-			std::memcpy(&r1[k * n], in + 2 + 2 * k * n + n, n * 4);
+			CK(cudaMemcpyAsync(h->b(ab_transform::REG0) + k * n, in + 2 + 2 * k * n, n * 4, cudaMemcpyHostToDevice, h->st));
+			CK(cudaMemcpyAsync(h->b(ab_transform::REG1) + k * n, in + 2 + 2 * k * n + n, n * 4, cudaMemcpyHostToDevice, h->st));
 		}
-		h->upload(ab_transform::REG0, r0.data());
-		h->upload(ab_transform::REG1, r1.data());
+		CK(cudaStreamSynchronize(h->st));
 		h->prefwd = false;
 	});
 }
+
+void * ab_host_alloc(size_t bytes)
+{
+	void * p = nullptr;
+	if (cudaMallocHost(&p, bytes) != cudaSuccess) { g_last_error = "cudaMallocHost failed"; return nullptr; }
+	return p;
+}
+
+void ab_host_free(void * p) { if (p) cudaFreeHost(p); }
 
 int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_words)
 {
@@ -635,6 +655,43 @@ int ab_timer_stop(ab_transform * h, float * ms)
 }
 
 const char * ab_last_error(void) { return g_last_error.c_str(); }
+
+int ab_launch_count(const ab_transform * h, uint64_t * count)
+{
+	return guarded([&] { if (h == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); *count = h->launches; });
+}
+
+int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * count)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (ms == nullptr || count == nullptr || cap < 1) throw ab_error(AB_E_ARG, "bad arguments");
+		if (h->prof.size() < (size_t)cap + 1)
+		{
+			for (cudaEvent_t e : h->prof) cudaEventDestroy(e);
+			h->prof.assign((size_t)cap + 1, nullptr);
+			for (auto & e : h->prof) CK(cudaEventCreate(&e));
+		}
+		h->prof_used = 0;                    // mark() records before every launch
+		h->square_mul((u32)a);
+		const size_t used = h->prof_used;
+		h->prof_used = h->prof.size();       // recording off
+		if (used == 0 || used > (size_t)cap) throw ab_error(AB_E_CAPACITY, "launch count exceeds cap");
+		CK(cudaEventRecord(h->prof[used], h->st));
+		CK(cudaEventSynchronize(h->prof[used]));
+		for (size_t i = 0; i < used; ++i) CK(cudaEventElapsedTime(&ms[i], h->prof[i], h->prof[i + 1]));
+		*count = (int)used;
+	});
+}
+
+int ab_flush_l2(ab_transform * h, size_t bytes)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (h->flush_buf == nullptr) CK(cudaMalloc(&h->flush_buf, bytes));
+		CK(cudaMemsetAsync(h->flush_buf, (int)(h->launches & 0xff), bytes, h->st));
+	});
+}
 
 int ab_diag_forward(ab_transform * h, int domain, const uint32_t * in, uint32_t * out)
 {

@@ -51,9 +51,10 @@ class Xoshiro256ss:
 
     def random_odd(self, bits):
         words = (bits + 63) // 64
-        x = 0
+        buf = bytearray(8 * words)
         for i in range(words):
-            x |= self.next() << (64 * i)
+            buf[8 * i:8 * i + 8] = self.next().to_bytes(8, "little")
+        x = int.from_bytes(bytes(buf), "little")
         x &= (1 << bits) - 1
         return x | (1 << (bits - 1)) | 1
 

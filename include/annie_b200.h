@@ -74,6 +74,10 @@ size_t ab_checkpoint_size(const ab_transform * h);
 int ab_save_checkpoint(ab_transform * h, void * buf, size_t cap, size_t * written);
 int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size);
 
+/* Page-locked host buffers for checkpoint payloads (DMA without staging). */
+void * ab_host_alloc(size_t bytes);
+void ab_host_free(void * p);
+
 /* Raw register words (K planes of n u32, normal form) -- the engine's
    read_memory / write_memory (engine.h of the reference). */
 int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_words);
@@ -93,6 +97,17 @@ int ab_timer_start(ab_transform * h);
 int ab_timer_stop(ab_transform * h, float * ms);
 
 const char * ab_last_error(void);
+
+/* Number of kernels this handle has launched (all entry points). */
+int ab_launch_count(const ab_transform * h, uint64_t * count);
+
+/* Runs one square_mul(a) with a CUDA event before every kernel launch and
+   returns each launch's device time (ms, launch order) in ms[0..*count). */
+int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * count);
+
+/* Overwrites a device buffer of `bytes` (allocated on first use) on the
+   handle's stream, evicting the transform's data from L2 (benchmarking). */
+int ab_flush_l2(ab_transform * h, size_t bytes);
 
 /* Diagnostics (kernel-level parity tests): run one stage on host data.
    ab_diag_forward:  full forward NTT of a normal-form register (domain 0 = R, 1 = Q).
