@@ -74,6 +74,7 @@ ABI = [
     ("ab_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
     ("ab_profile_square", [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)], C.c_int),
     ("ab_flush_l2", [C.c_void_p, C.c_size_t], C.c_int),
+    ("ab_square_mul_noalloc", [C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
     ("ab_diag_product", [C.c_void_p, C.c_int, _u32p, _u32p, C.c_uint32, _u32p, C.c_int, _u32p], C.c_int),
 ]
@@ -254,6 +255,10 @@ class Transform:
 
     def flush_l2(self, nbytes=256 << 20):
         _check(self.L.ab_flush_l2(self.h, nbytes))
+
+    def square_mul_noalloc(self, device_ptr, a):
+        """square_mul on a caller-owned device register (K*n u32), no allocation."""
+        _check(self.L.ab_square_mul_noalloc(self.h, C.c_void_p(device_ptr), a))
 
     # -- information strings (transformGPU.h:766-795)
     def get_info_short(self):

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <stdexcept>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "gmp.h"
@@ -441,6 +442,40 @@ struct ab_transform
 	}
 };
 
+// ============================================================ allocation-free squaring
+// Work buffers of ab_square_mul_noalloc: five registers of at most
+// AB_NOALLOC_MAX_WORDS words each (10 MiB), in a static device array that
+// every GPU loading this library holds until the process exits.  Host code
+// cannot use the symbol as an address: the device address is fetched once
+// per device with cudaGetSymbolAddress, with that device current.
+#define AB_NOALLOC_MAX_WORDS (1u << 19)
+#define AB_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) u32 g_noalloc_scratch[5 * AB_NOALLOC_MAX_WORDS];
+
+namespace
+{
+std::mutex g_noalloc_mu;
+u32 * g_noalloc_addr[AB_NOALLOC_MAX_DEVICES] = {};
+
+u32 * noalloc_scratch(int device)
+{
+	if (device < 0 || device >= AB_NOALLOC_MAX_DEVICES) throw ab_error(AB_E_ARG, "device index out of range");
+	std::lock_guard<std::mutex> lock(g_noalloc_mu);
+	if (g_noalloc_addr[device] == nullptr)
+	{
+		int prev = 0;
+		CK(cudaGetDevice(&prev));
+		CK(cudaSetDevice(device));
+		void * p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		cudaSetDevice(prev);
+		if (e != cudaSuccess) throw ab_error(AB_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+		g_noalloc_addr[device] = static_cast<u32 *>(p);
+	}
+	return g_noalloc_addr[device];
+}
+}
+
 // ============================================================ C ABI
 namespace
 {
@@ -690,6 +725,36 @@ int ab_flush_l2(ab_transform * h, size_t bytes)
 		need_ready(h);
 		if (h->flush_buf == nullptr) CK(cudaMalloc(&h->flush_buf, bytes));
 		CK(cudaMemsetAsync(h->flush_buf, (int)(h->launches & 0xff), bytes, h->st));
+	});
+}
+
+int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg, int32_t a)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (reg == nullptr) throw ab_error(AB_E_ARG, "null register");
+		const size_t words = (size_t)h->prm.K * h->n;
+		if (words > AB_NOALLOC_MAX_WORDS)
+			throw ab_error(AB_E_CAPACITY, "ab_square_mul_noalloc: K*n = " + std::to_string(words) +
+				" words exceeds the static scratch limit of " + std::to_string(AB_NOALLOC_MAX_WORDS) + " words per register");
+		u32 * const s = noalloc_scratch(h->device);
+		u32 * const aq0 = s, * const ar0 = s + AB_NOALLOC_MAX_WORDS, * const aq1 = s + 2 * AB_NOALLOC_MAX_WORDS;
+		u32 * const ar1 = s + 3 * AB_NOALLOC_MAX_WORDS, * const tq = s + 4 * AB_NOALLOC_MAX_WORDS;
+		using T = ab_transform;
+		const u32 * wq = h->b(T::WQ), * wr = h->b(T::WR);
+		// squareMMGW (transformGPU.h:556-568) with every intermediate in the
+		// static scratch: each scratch word is written before it is read
+		// within the call, so nothing needs clearing between calls
+		ColJob j0 = h->cj_norm(reg); T::set_fwd(j0, aq0, wq, ar0, wr); h->cols(j0);
+		RowJob rq = h->rj(aq0, ROW_SQUARE, wq), rr = h->rj(ar0, ROW_SQUARE, wr);
+		h->rows(rq, &rr);
+		ColJob jq = h->cj_tr(aq0, wq, (u32)a, 1, nullptr, LOWER_NONE); jq.out_norm = tq;
+		ColJob jr = h->cj_tr(ar0, wr, (u32)a, 0, nullptr, LOWER_NONE); T::set_fwd(jr, nullptr, nullptr, ar1, wr);
+		h->cols(jq, &jr);
+		h->rows(h->rj(ar1, ROW_MUL, wr, h->b(T::NIR)));
+		ColJob j1 = h->cj_tr(ar1, wr, 1, 0, nullptr, LOWER_R_ADD2); T::set_fwd(j1, aq1, wq, nullptr, nullptr); h->cols(j1);
+		h->rows(h->rj(aq1, ROW_MUL, wq, h->b(T::NQ)));
+		ColJob j2 = h->cj_tr(aq1, wq, 1, 1, tq, LOWER_Q); j2.out_norm = reg; h->cols(j2);
 	});
 }
 

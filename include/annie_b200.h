@@ -109,6 +109,26 @@ int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * co
    handle's stream, evicting the transform's data from L2 (benchmarking). */
 int ab_flush_l2(ab_transform * h, size_t bytes);
 
+/* Allocation-free square_mul -- no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory once they are running: code
+ * inside a stream capture (cudaMalloc is not capturable), a host that hands
+ * all device memory to its own allocator or pool at start-up, or a service
+ * with a fixed memory budget.  Such a caller creates the handle (which
+ * allocates) during start-up, and afterwards squares registers it owns:
+ * reg_device = a caller-owned device array of K*n words in the normal
+ * register layout; it is replaced by a * reg^2 in MMGW form, exactly as
+ * ab_square_mul does for Reg0.  The work buffers come from a static device
+ * array of 5 x 2^19 words (10 MiB) that every GPU loading this library holds
+ * until exit, so K*n must not exceed 2^19 words (else AB_E_CAPACITY).  No
+ * cudaMalloc, cudaFree or allocating library call is made.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress, with
+ * that device current); make that first call before any stream capture.
+ * Work is queued on the handle's stream (ab_synchronize waits for it).  All
+ * calls share the one array: calls whose work overlaps on the GPU (other
+ * handles' streams, other host threads) race and give wrong results. */
+int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg_device, int32_t a);
+
 /* Diagnostics (kernel-level parity tests): run one stage on host data.
    ab_diag_forward:  full forward NTT of a normal-form register (domain 0 = R, 1 = Q).
    ab_diag_product:  forward NTT, pointwise square (xp == NULL) or product with the
