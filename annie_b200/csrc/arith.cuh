@@ -140,21 +140,35 @@ __device__ __forceinline__ Big<K> big_mul_u32(const Big<K> & a, u32 y)
 template <int K>
 __device__ __forceinline__ bool big_is_neg(const Big<K> & a) { return (a.l[K - 1] >> 31) != 0; }
 
-// arithmetic right shift by s, 0 < s < 32K
+// arithmetic right shift by s, 0 < s < 32K.  s is the same in every thread
+// (it derives from the digit size), so the limb move is a uniform branch and
+// only the sub-limb part is a funnel shift.
 template <int K>
 __device__ __forceinline__ Big<K> big_sar(const Big<K> & a, int s)
 {
 	const u32 fill = big_is_neg<K>(a) ? 0xffffffffu : 0u;
-	const int ws = s >> 5, bs = s & 31;
-	Big<K> r;
+	u32 t[K + 1];
 #pragma unroll
-	for (int i = 0; i < K; ++i)
+	for (int i = 0; i < K; ++i) t[i] = a.l[i];
+	t[K] = fill;
+	int ws = s >> 5;
+	while (ws > 0)
 	{
-		const int i0 = i + ws, i1 = i + ws + 1;
-		u32 lo = fill, hi = fill;
 #pragma unroll
-		for (int j = 0; j < K; ++j) { if (j == i0) lo = a.l[j]; if (j == i1) hi = a.l[j]; }
-		r.l[i] = (bs == 0) ? lo : __funnelshift_r(lo, hi, bs);
+		for (int i = 0; i < K; ++i) t[i] = t[i + 1];
+		--ws;
+	}
+	const int bs = s & 31;
+	Big<K> r;
+	if (bs == 0)
+	{
+#pragma unroll
+		for (int i = 0; i < K; ++i) r.l[i] = t[i];
+	}
+	else
+	{
+#pragma unroll
+		for (int i = 0; i < K; ++i) r.l[i] = __funnelshift_r(t[i], t[i + 1], bs);
 	}
 	return r;
 }

@@ -160,7 +160,9 @@ struct ab_transform
 
 	int device = 0;
 	cudaStream_t st = nullptr;
-	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	cudaStream_t st2 = nullptr;          // Q-domain chain, joined before the carry-sub
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_q = nullptr;
+	bool overlap = true;                 // run the Q chain on st2 (off for per-launch profiling)
 	ab_params prm{};
 	size_t n = 0;
 	Geometry geo{};
@@ -184,6 +186,9 @@ struct ab_transform
 		if (dmem) cudaFree(dmem);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
+		if (ev_fork) cudaEventDestroy(ev_fork);
+		if (ev_q) cudaEventDestroy(ev_q);
+		if (st2) cudaStreamDestroy(st2);
 		if (st) cudaStreamDestroy(st);
 		mpz_clears(N, factor, nullptr);
 	}
@@ -286,18 +291,18 @@ struct ab_transform
 	{
 		if (prof_used < prof.size()) CK(cudaEventRecord(prof[prof_used++], st));
 	}
-	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
+	void rows(const RowJob & j0, const RowJob * j1 = nullptr, cudaStream_t s = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
-		mark();
-		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st));
+		if (s == nullptr) { mark(); s = st; }
+		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, s));
 		++launches;
 	}
-	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
+	void cols(const ColJob & j0, const ColJob * j1 = nullptr, cudaStream_t s = nullptr)
 	{
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
-		mark();
-		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st));
+		if (s == nullptr) { mark(); s = st; }
+		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, s));
 		++launches;
 	}
 	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp = nullptr) const
@@ -331,26 +336,51 @@ struct ab_transform
 
 	// reduceMMGW tail (transformGPU.h:523-538): m' = T_R Ninv mod R, +2,
 	// r' = m' N - T_Q mod Q.  AR1 holds the first forward levels of T_R.
-	void reduce_tail(const u32 * tq, u32 * out, bool want_prefwd)
+	void reduce_tail(const u32 * tq, u32 * out, bool want_prefwd, bool join_q = false)
 	{
 		rows(rj(b(AR1), ROW_MUL, b(WR), b(NIR)));
 		ColJob j1 = cj_tr(b(AR1), b(WR), 1, 0, nullptr, LOWER_R_ADD2); set_fwd(j1, b(AQ1), b(WQ), nullptr, nullptr); cols(j1);
 		rows(rj(b(AQ1), ROW_MUL, b(WQ), b(NQ)));
+		if (join_q) CK(cudaStreamWaitEvent(st, ev_q, 0));
 		ColJob j2 = cj_tr(b(AQ1), b(WQ), 1, 1, tq, LOWER_Q); j2.out_norm = out;
 		if (want_prefwd) set_fwd(j2, b(AQ0), b(WQ), b(AR0), b(WR));
 		cols(j2);
+	}
+
+	// First product of squareMMGW / mulMMGW (transformGPU.h:540-568):
+	// T_Q = carry(x y mod Q) into TQ and the first forward levels of
+	// carry(x y mod R) into AR1.  AQ0/AR0 hold the first forward levels of x;
+	// xq/xr the full forward images of y (nullptr: y = x, square).  With
+	// overlap, the Q chain runs on st2 (T_Q is only needed by the final
+	// carry-sub) and reduce_tail joins it.
+	void first_product(u32 a, const u32 * xq, const u32 * xr)
+	{
+		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, b(WQ), xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, b(WR), xr);
+		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
+		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
+		if (overlap)
+		{
+			CK(cudaEventRecord(ev_fork, st));
+			CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+			rows(rq, nullptr, st2);
+			cols(jq, nullptr, st2);
+			CK(cudaEventRecord(ev_q, st2));
+			rows(rr);
+			cols(jr);
+		}
+		else
+		{
+			rows(rq, &rr);
+			cols(jq, &jr);
+		}
 	}
 
 	// squareMMGW (transformGPU.h:556-568)
 	void square_mul(u32 a)
 	{
 		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
-		RowJob rq = rj(b(AQ0), ROW_SQUARE, b(WQ)), rr = rj(b(AR0), ROW_SQUARE, b(WR));
-		rows(rq, &rr);
-		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
-		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
-		cols(jq, &jr);
-		reduce_tail(b(TQ), b(REG0), true);
+		first_product(a, nullptr, nullptr);
+		reduce_tail(b(TQ), b(REG0), true, overlap);
 		prefwd = true;
 	}
 
@@ -360,12 +390,8 @@ struct ab_transform
 		full_forward(b(src), b(OPQ), b(OPR));
 		{ ColJob j = cj_norm(b(dst)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
 		prefwd = false;
-		RowJob rq = rj(b(AQ0), ROW_MUL, b(WQ), b(OPQ)), rr = rj(b(AR0), ROW_MUL, b(WR), b(OPR));
-		rows(rq, &rr);
-		ColJob jq = cj_tr(b(AQ0), b(WQ), 1, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
-		ColJob jr = cj_tr(b(AR0), b(WR), 1, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
-		cols(jq, &jr);
-		reduce_tail(b(TQ), b(dst), dst == REG0);
+		first_product(1, b(OPQ), b(OPR));
+		reduce_tail(b(TQ), b(dst), dst == REG0, overlap);
 		prefwd = (dst == REG0);
 	}
 
@@ -418,7 +444,10 @@ struct ab_transform
 
 		CK(cudaSetDevice(device));
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
 		CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
+		CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+		CK(cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming));
 		CK(cudaMalloc(&dmem, (size_t)NBUF * prm.K * n * 4));
 		CK(cudaMemsetAsync(dmem, 0, (size_t)NBUF * prm.K * n * 4, st));
 
@@ -708,7 +737,10 @@ int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * co
 			for (auto & e : h->prof) CK(cudaEventCreate(&e));
 		}
 		h->prof_used = 0;                    // mark() records before every launch
+		const bool ov = h->overlap;
+		h->overlap = false;                  // one stream: launches in order
 		h->square_mul((u32)a);
+		h->overlap = ov;
 		const size_t used = h->prof_used;
 		h->prof_used = h->prof.size();       // recording off
 		if (used == 0 || used > (size_t)cap) throw ab_error(AB_E_CAPACITY, "launch count exceeds cap");

@@ -37,157 +37,150 @@ __device__ __forceinline__ void inv_bfly(u32 & x0, u32 & x1, u32 wi, u32 wiq, u3
 	x1 = mont_mul_c(t, wi, wiq, p);
 }
 
-// shared-memory index with one pad word per 32: conflict-free for both the
-// strided stage layouts and the 32-consecutive-per-thread layout
-__device__ __forceinline__ u32 padx(u32 e) { return e + (e >> 5); }
-
 // ================================================================ row pass
-// Stage plan for a row of R = 2^(LB+1) words (levels t = 0..LB-1 touch bit
-// LB-t of the in-row index): the last stage owns bits 4..1 plus the pair bit
-// 0 (32 consecutive words per thread); the LB-4 levels above are split into
-// stages of at most 5 levels.
-template <int LB>
-struct RowPlan
-{
-	static constexpr int NL = LB - 4;
-	static constexpr int NS = (NL + 4) / 5;
-	__host__ __device__ static constexpr int size(int i) { return (NS == 0) ? 0 : NL / NS + ((i < NL % NS) ? 1 : 0); }
-	__host__ __device__ static constexpr int blo(int i)
-	{
-		int b = LB + 1;
-		for (int k = 0; k <= i; ++k) b -= size(k);
-		return b;
-	}
-};
+// A CTA transforms one row (R = 2^(LB+1) words) of one prime: levels
+// t = 0..LB-1 of the row touch bit LB-t of the in-row index.  Each thread
+// holds 16 words; a stage applies S <= 4 levels to groups of 2^S words in
+// registers, and stages exchange through shared memory.  The last stage owns
+// bits 4..1; bit 0 (the two halves of a degree-1 polynomial) comes from the
+// thread index, so the pointwise product pairs lane 2m with lane 2m+1.
+// Stage loops are rolled (runtime bit positions) to keep the code small.
+constexpr int RP_EPT = 16;
 
-// element of a non-last stage: group bits g (S of them) at bit BLO, the other
-// bits from o = tid + T*x
-template <int S, int BLO, u32 T>
-__device__ __forceinline__ u32 stage_elem(u32 tid, int x, int g)
+// element of a stage with S group bits at bit b; the other bits come from
+// o = tid + T*x (x selects one of the 16 / 2^S groups of the thread)
+__device__ __forceinline__ u32 rp_elem(u32 tid, u32 T, int x, int S, int b, int g)
 {
 	const u32 o = tid + T * (u32)x;
-	return (o & ((1u << BLO) - 1)) | ((u32)g << BLO) | ((o >> BLO) << (BLO + S));
+	return (o & ((1u << b) - 1)) | ((u32)g << b) | ((o >> b) << (b + S));
 }
 
-template <int LB, int S, int BLO, bool INV>
-__device__ __forceinline__ void row_stage(u32 (&v)[32], u32 tid, const u32 * __restrict__ w, u32 Hr, u32 p, u32 q)
+// two pad words per 32: conflict-free for every stage layout, including the
+// last one (lanes 2m, 2m+1 at elements 32m + {0,1} + 2g)
+__device__ __forceinline__ u32 rp_pad(u32 e) { return e + ((e >> 5) << 1); }
+
+template <int S, bool INV, bool SAVE>
+__device__ __forceinline__ void rp_radix(u32 (&v)[RP_EPT], u32 tid, u32 T, int b, int LB, const u32 * __restrict__ w,
+	u32 Hr, u32 p, u32 q, u32 (&w1)[8], u32 (&w1q)[8])
 {
-	constexpr int G = 32 >> S;
-	constexpr u32 T = (1u << (LB + 1)) / 32;
+	constexpr int G = RP_EPT >> S;
 #pragma unroll
 	for (int x = 0; x < G; ++x)
 	{
-		const u32 ohi = (tid + T * (u32)x) >> BLO;
+		const u32 ohi = (tid + T * (u32)x) >> b;
 #pragma unroll
 		for (int ss = 0; ss < S; ++ss)
 		{
 			const int s = INV ? ss : (S - 1 - ss);
-			const int t = LB - BLO - s;
+			const int t = LB - b - s;
+			const u32 * __restrict__ wl = w + ((Hr << t) + (ohi << (S - 1 - s)));
 #pragma unroll
 			for (int jh = 0; jh < (1 << (S - 1 - s)); ++jh)
 			{
-				const u32 jj = (u32)jh + (ohi << (S - 1 - s));
-				const u32 wv = __ldg(&w[(Hr << t) + jj]);
+				const u32 wv = __ldg(wl + jh);
 				const u32 wq = wv * q;
+				if (SAVE && s == 0) { w1[jh] = wv; w1q[jh] = wq; }
 #pragma unroll
 				for (int gl = 0; gl < (1 << s); ++gl)
 				{
-					const int g = (jh << (s + 1)) + gl;
-					if (INV) inv_bfly(v[x * (1 << S) + g], v[x * (1 << S) + g + (1 << s)], wv, wq, p);
-					else fwd_bfly(v[x * (1 << S) + g], v[x * (1 << S) + g + (1 << s)], wv, wq, p);
+					const int g = x * (1 << S) + (jh << (s + 1)) + gl;
+					if (INV) inv_bfly(v[g], v[g + (1 << s)], wv, wq, p);
+					else fwd_bfly(v[g], v[g + (1 << s)], wv, wq, p);
 				}
 			}
 		}
 	}
 }
 
-template <int S, int BLO, u32 T>
-__device__ __forceinline__ void stage_load_smem(u32 (&v)[32], const u32 * sm, u32 tid)
+// Stage addressing: the 2^S words of a group are e0 + g 2^b.  In the padded
+// shared layout they are pad(e0) + g D with D = 2^b + 2^(b-4) for b >= 5, and
+// D = 2 for the last stage (b = 1, the group stays inside one 32-word block).
+__device__ __forceinline__ u32 rp_base(u32 tid, u32 T, int x, int S, int b)
 {
-#pragma unroll
-	for (int x = 0; x < (32 >> S); ++x)
-#pragma unroll
-		for (int g = 0; g < (1 << S); ++g) v[x * (1 << S) + g] = sm[padx(stage_elem<S, BLO, T>(tid, x, g))];
+	const u32 o = tid + T * (u32)x;
+	return (o & ((1u << b) - 1)) | ((o >> b) << (b + S));
 }
+__device__ __forceinline__ u32 rp_step(int b) { return (b >= 5) ? (1u << b) + (1u << (b - 4)) : (1u << b); }
 
-template <int S, int BLO, u32 T>
-__device__ __forceinline__ void stage_store_smem(const u32 (&v)[32], u32 * sm, u32 tid)
+template <int S>
+__device__ __forceinline__ void rp_load_smem(u32 (&v)[RP_EPT], const u32 * sm, u32 tid, u32 T, int b)
 {
+	const u32 D = rp_step(b);
 #pragma unroll
-	for (int x = 0; x < (32 >> S); ++x)
-#pragma unroll
-		for (int g = 0; g < (1 << S); ++g) sm[padx(stage_elem<S, BLO, T>(tid, x, g))] = v[x * (1 << S) + g];
-}
-
-template <int S, int BLO, u32 T>
-__device__ __forceinline__ void stage_load_global(u32 (&v)[32], const u32 * __restrict__ x, u32 tid)
-{
-#pragma unroll
-	for (int xx = 0; xx < (32 >> S); ++xx)
-#pragma unroll
-		for (int g = 0; g < (1 << S); ++g) v[xx * (1 << S) + g] = x[stage_elem<S, BLO, T>(tid, xx, g)];
-}
-
-template <int S, int BLO, u32 T>
-__device__ __forceinline__ void stage_store_global(const u32 (&v)[32], u32 * __restrict__ x, u32 tid)
-{
-#pragma unroll
-	for (int xx = 0; xx < (32 >> S); ++xx)
-#pragma unroll
-		for (int g = 0; g < (1 << S); ++g) x[stage_elem<S, BLO, T>(tid, xx, g)] = v[xx * (1 << S) + g];
-}
-
-// last stage: v[i] = row element tid*32 + i; levels on bits 4..1
-template <int LB, bool INV>
-__device__ __forceinline__ void row_last(u32 (&v)[32], u32 tid, const u32 * __restrict__ w, u32 Hr, u32 p, u32 q,
-	u32 (&w1)[8], u32 (&w1q)[8])
-{
-#pragma unroll
-	for (int bb = 0; bb < 4; ++bb)
+	for (int x = 0; x < (RP_EPT >> S); ++x)
 	{
-		const int b = INV ? (1 + bb) : (4 - bb);
-		const int t = LB - b;
+		const u32 * a = sm + rp_pad(rp_base(tid, T, x, S, b));
 #pragma unroll
-		for (int jh = 0; jh < (16 >> b); ++jh)
-		{
-			const u32 jj = (tid << (4 - b)) + (u32)jh;
-			const u32 wv = __ldg(&w[(Hr << t) + jj]);
-			const u32 wq = wv * q;
-			if (!INV && b == 1) { w1[jh] = wv; w1q[jh] = wq; }
-#pragma unroll
-			for (int gl = 0; gl < (1 << b); ++gl)
-			{
-				const int i = (jh << (b + 1)) + gl;
-				if (INV) inv_bfly(v[i], v[i + (1 << b)], wv, wq, p);
-				else fwd_bfly(v[i], v[i + (1 << b)], wv, wq, p);
-			}
-		}
+		for (int g = 0; g < (1 << S); ++g) v[x * (1 << S) + g] = a[g * D];
 	}
 }
 
-// pointwise product of the 16 degree-1 polynomials held by the thread
-__device__ __forceinline__ void row_pointwise(u32 (&v)[32], const u32 * __restrict__ xp, bool is_mul,
+template <int S>
+__device__ __forceinline__ void rp_store_smem(const u32 (&v)[RP_EPT], u32 * sm, u32 tid, u32 T, int b)
+{
+	const u32 D = rp_step(b);
+#pragma unroll
+	for (int x = 0; x < (RP_EPT >> S); ++x)
+	{
+		u32 * a = sm + rp_pad(rp_base(tid, T, x, S, b));
+#pragma unroll
+		for (int g = 0; g < (1 << S); ++g) a[g * D] = v[x * (1 << S) + g];
+	}
+}
+
+template <int S>
+__device__ __forceinline__ void rp_load_global(u32 (&v)[RP_EPT], const u32 * __restrict__ x, u32 tid, u32 T, int b)
+{
+#pragma unroll
+	for (int xx = 0; xx < (RP_EPT >> S); ++xx)
+	{
+		const u32 * a = x + rp_base(tid, T, xx, S, b);
+#pragma unroll
+		for (int g = 0; g < (1 << S); ++g) v[xx * (1 << S) + g] = a[(u32)g << b];
+	}
+}
+
+template <int S>
+__device__ __forceinline__ void rp_store_global(const u32 (&v)[RP_EPT], u32 * __restrict__ x, u32 tid, u32 T, int b)
+{
+#pragma unroll
+	for (int xx = 0; xx < (RP_EPT >> S); ++xx)
+	{
+		u32 * a = x + rp_base(tid, T, xx, S, b);
+#pragma unroll
+		for (int g = 0; g < (1 << S); ++g) a[(u32)g << b] = v[xx * (1 << S) + g];
+	}
+}
+
+// Pointwise product of the degree-1 polynomials (x0, x1) mod (x^2 -+ c):
+// lane 2m holds the x0 of the thread pair's 16 polynomials, lane 2m+1 the x1.
+// Each lane computes 8 whole products (even lane: slots 0..7, odd: 8..15).
+__device__ __forceinline__ void rp_pointwise(u32 (&v)[RP_EPT], const u32 * __restrict__ xp, bool is_mul, u32 tid, u32 NT,
 	const u32 (&w1)[8], const u32 (&w1q)[8], u32 p, u32 q)
 {
-	u32 pv[32];
+	// tid: virtual thread (its 16 words are the last-stage elements
+	// 32*(tid>>1) + (tid&1) + 2g); NT: physical threads of the CTA (warp mask)
+	const bool odd = (tid & 1) != 0;
+	const unsigned mask = (NT >= 32) ? 0xffffffffu : ((1u << NT) - 1);
+	u32 pv[RP_EPT];
 	if (is_mul)
 	{
 #pragma unroll
-		for (int i = 0; i < 8; ++i)
-		{
-			const uint4 t = __ldg(reinterpret_cast<const uint4 *>(xp) + i);
-			pv[4 * i] = t.x; pv[4 * i + 1] = t.y; pv[4 * i + 2] = t.z; pv[4 * i + 3] = t.w;
-		}
+		for (int i = 0; i < RP_EPT; ++i) pv[i] = __ldg(&xp[(tid & 1) + 2 * i + ((tid >> 1) << 5)]);
 	}
 #pragma unroll
-	for (int m = 0; m < 16; ++m)
+	for (int i = 0; i < 8; ++i)
 	{
-		const u32 x0 = v[2 * m], x1 = v[2 * m + 1];
-		const u32 cw = w1[m >> 1], cq = w1q[m >> 1];
+		const u32 r = __shfl_xor_sync(mask, odd ? v[i] : v[8 + i], 1);
+		const u32 x0 = odd ? r : v[i], x1 = odd ? v[8 + i] : r;
+		const int slot = odd ? 8 + i : i;   // polynomial slot; parity = sign
+		const u32 cw = odd ? w1[4 + (i >> 1)] : w1[i >> 1];
+		const u32 cq = odd ? w1q[4 + (i >> 1)] : w1q[i >> 1];
 		u32 t, y0, y1;
 		if (is_mul)
 		{
-			const u32 p0 = pv[2 * m], p1 = pv[2 * m + 1];
+			const u32 rp2 = __shfl_xor_sync(mask, odd ? pv[i] : pv[8 + i], 1);
+			const u32 p0 = odd ? rp2 : pv[i], p1 = odd ? pv[8 + i] : rp2;
 			t = mont_mul_c(mont_mul(x1, p1, p, q), cw, cq, p);
 			y1 = add_mod(mont_mul(x0, p1, p, q), mont_mul(p0, x1, p, q), p);
 			y0 = mont_mul(x0, p0, p, q);
@@ -198,17 +191,33 @@ __device__ __forceinline__ void row_pointwise(u32 (&v)[32], const u32 * __restri
 			y1 = mont_mul(add_mod(x0, x0, p), x1, p, q);
 			y0 = mont_mul(x0, x0, p, q);
 		}
-		v[2 * m] = ((m & 1) == 0) ? add_mod(y0, t, p) : sub_mod(y0, t, p);
-		v[2 * m + 1] = y1;
+		y0 = ((slot & 1) == 0) ? add_mod(y0, t, p) : sub_mod(y0, t, p);
+		const u32 r2 = __shfl_xor_sync(mask, odd ? y0 : y1, 1);
+		if (odd) { v[8 + i] = y1; v[i] = r2; }
+		else { v[i] = y0; v[8 + i] = r2; }
 	}
 }
 
+// Physical threads of a row-pass CTA: 16 words per virtual thread, at most
+// 256 threads, each running R / (16 * threads) rounds per stage -- so that
+// every CTA of a launch is resident at once (3 CTAs per SM).
 template <int LOG_R>
-__global__ void __launch_bounds__((1 << LOG_R) / 32) k_rowpass(const RowJobs jobs, const TConst c)
+struct RowCfg
+{
+	static constexpr u32 T = (1u << LOG_R) / RP_EPT;             // virtual threads
+	static constexpr u32 NT = (T < 256u) ? T : 256u;             // physical threads
+	static constexpr u32 RND = T / NT;
+};
+
+template <int LOG_R>
+__global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 3) k_rowpass(const RowJobs jobs, const TConst c)
 {
 	constexpr int LB = LOG_R - 1;
-	constexpr u32 T = (1u << LOG_R) / 32;
-	using P = RowPlan<LB>;
+	constexpr u32 T = RowCfg<LOG_R>::T, NT = RowCfg<LOG_R>::NT, RND = RowCfg<LOG_R>::RND;
+	constexpr int NL = LB - 4;                                    // levels above the last stage
+	constexpr int S0 = (NL % 4 == 0) ? 4 : NL % 4;                // first stage (when NL > 0)
+	constexpr int NS = (NL == 0) ? 0 : 1 + (NL - S0) / 4;        // stages above the last
+	constexpr int B0 = LB + 1 - S0;
 	extern __shared__ __align__(16) u32 sm[];
 
 	const RowJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
@@ -217,128 +226,191 @@ __global__ void __launch_bounds__((1 << LOG_R) / 32) k_rowpass(const RowJobs job
 	u32 * __restrict__ x = J.x + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
 	const u32 * __restrict__ w = J.w + (size_t)k * c.n;
 	const u32 * __restrict__ wi = w + (c.n >> 1);
+	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
 	const u32 Hr = c.H + r;
 	const u32 tid = threadIdx.x;
-	u32 v[32];
+	u32 v[RP_EPT];
 	u32 w1[8], w1q[8];
 
-	// ---- forward
-	if constexpr (P::NS == 0)
+	if constexpr (NS == 0)
 	{
-#pragma unroll
-		for (int i = 0; i < 8; ++i)
+#pragma unroll 1
+		for (u32 rr = 0; rr < RND; ++rr)
 		{
-			const uint4 t = reinterpret_cast<const uint4 *>(x + tid * 32)[i];
-			v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+			const u32 vt = tid + rr * NT;
+			rp_load_global<4>(v, x, vt, T, 1);
+			rp_radix<4, false, true>(v, vt, T, 1, LB, w, Hr, p, q, w1, w1q);
+			if (J.mode != ROW_FWD_ONLY)
+			{
+				rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1, w1q, p, q);
+				rp_radix<4, true, false>(v, vt, T, 1, LB, wi, Hr, p, q, w1, w1q);
+			}
+			rp_store_global<4>(v, x, vt, T, 1);
 		}
-	}
-	else
-	{
-		constexpr int S0 = P::size(0), B0 = P::blo(0);
-		stage_load_global<S0, B0, T>(v, x, tid);
-		row_stage<LB, S0, B0, false>(v, tid, w, Hr, p, q);
-		stage_store_smem<S0, B0, T>(v, sm, tid);
-		__syncthreads();
-		if constexpr (P::NS >= 2)
-		{
-			constexpr int S1 = P::size(1), B1 = P::blo(1);
-			stage_load_smem<S1, B1, T>(v, sm, tid);
-			row_stage<LB, S1, B1, false>(v, tid, w, Hr, p, q);
-			stage_store_smem<S1, B1, T>(v, sm, tid);
-			__syncthreads();
-		}
-#pragma unroll
-		for (int i = 0; i < 32; ++i) v[i] = sm[padx(tid * 32 + i)];
-	}
-	row_last<LB, false>(v, tid, w, Hr, p, q, w1, w1q);
-
-	if (J.mode == ROW_FWD_ONLY)
-	{
-#pragma unroll
-		for (int i = 0; i < 8; ++i)
-			reinterpret_cast<uint4 *>(x + tid * 32)[i] = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
 		return;
 	}
-
-	// ---- pointwise
-	row_pointwise(v, (J.mode == ROW_MUL) ? J.xp + (size_t)k * c.n + (size_t)r * (1u << LOG_R) + tid * 32 : nullptr,
-		J.mode == ROW_MUL, w1, w1q, p, q);
-
-	// ---- inverse
-	row_last<LB, true>(v, tid, wi, Hr, p, q, w1, w1q);
-	if constexpr (P::NS == 0)
-	{
-#pragma unroll
-		for (int i = 0; i < 8; ++i)
-			reinterpret_cast<uint4 *>(x + tid * 32)[i] = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-	}
 	else
 	{
-#pragma unroll
-		for (int i = 0; i < 32; ++i) sm[padx(tid * 32 + i)] = v[i];
-		__syncthreads();
-		if constexpr (P::NS >= 2)
+		// ---- forward: stage 0 from global, then stages of 4 levels via smem
+#pragma unroll 1
+		for (u32 rr = 0; rr < RND; ++rr)
 		{
-			constexpr int S1 = P::size(1), B1 = P::blo(1);
-			stage_load_smem<S1, B1, T>(v, sm, tid);
-			row_stage<LB, S1, B1, true>(v, tid, wi, Hr, p, q);
-			stage_store_smem<S1, B1, T>(v, sm, tid);
-			__syncthreads();
+			const u32 vt = tid + rr * NT;
+			rp_load_global<S0>(v, x, vt, T, B0);
+			rp_radix<S0, false, false>(v, vt, T, B0, LB, w, Hr, p, q, w1, w1q);
+			rp_store_smem<S0>(v, sm, vt, T, B0);
 		}
-		constexpr int S0 = P::size(0), B0 = P::blo(0);
-		stage_load_smem<S0, B0, T>(v, sm, tid);
-		row_stage<LB, S0, B0, true>(v, tid, wi, Hr, p, q);
-		stage_store_global<S0, B0, T>(v, x, tid);
+		int b = B0;
+#pragma unroll 1
+		for (int i = 1; i < NS; ++i)
+		{
+			__syncthreads();
+			b -= 4;
+#pragma unroll 1
+			for (u32 rr = 0; rr < RND; ++rr)
+			{
+				const u32 vt = tid + rr * NT;
+				rp_load_smem<4>(v, sm, vt, T, b);
+				rp_radix<4, false, false>(v, vt, T, b, LB, w, Hr, p, q, w1, w1q);
+				rp_store_smem<4>(v, sm, vt, T, b);
+			}
+		}
+		__syncthreads();
+
+		// ---- last stage (bits 4..1), pointwise, inverse last stage
+#pragma unroll 1
+		for (u32 rr = 0; rr < RND; ++rr)
+		{
+			const u32 vt = tid + rr * NT;
+			rp_load_smem<4>(v, sm, vt, T, 1);
+			rp_radix<4, false, true>(v, vt, T, 1, LB, w, Hr, p, q, w1, w1q);
+			if (J.mode == ROW_FWD_ONLY)
+			{
+				rp_store_global<4>(v, x, vt, T, 1);
+				continue;
+			}
+			rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1, w1q, p, q);
+			rp_radix<4, true, false>(v, vt, T, 1, LB, wi, Hr, p, q, w1, w1q);
+			rp_store_smem<4>(v, sm, vt, T, 1);
+		}
+		if (J.mode == ROW_FWD_ONLY) return;
+
+		// ---- inverse: back up through smem, stage 0 to global
+		b = 1;
+#pragma unroll 1
+		for (int i = NS - 1; i >= 1; --i)
+		{
+			__syncthreads();
+			b += 4;
+#pragma unroll 1
+			for (u32 rr = 0; rr < RND; ++rr)
+			{
+				const u32 vt = tid + rr * NT;
+				rp_load_smem<4>(v, sm, vt, T, b);
+				rp_radix<4, true, false>(v, vt, T, b, LB, wi, Hr, p, q, w1, w1q);
+				rp_store_smem<4>(v, sm, vt, T, b);
+			}
+		}
+		__syncthreads();
+#pragma unroll 1
+		for (u32 rr = 0; rr < RND; ++rr)
+		{
+			const u32 vt = tid + rr * NT;
+			rp_load_smem<S0>(v, sm, vt, T, B0);
+			rp_radix<S0, true, false>(v, vt, T, B0, LB, wi, Hr, p, q, w1, w1q);
+			rp_store_global<S0>(v, x, vt, T, B0);
+		}
 	}
 }
 
 // ================================================================ column pass
 constexpr int CC = 32;  // own columns per CTA
+constexpr int COL_THREADS = 384;
 constexpr int TW = 40;  // tile row stride: own columns + up to 8 predecessor columns
 
-template <int LOG_H>
-__device__ __forceinline__ void col_inv(u32 (&v)[1 << LOG_H], const u32 * wi, u32 p, u32 q)
+// One radix-2^S step of the column transform (levels on row bits b..b+S-1)
+// for one column of one prime: the 2^S rows that differ in those bits.
+// Global level l (2^l polynomials) works on row bit LOG_H-1-l with twiddle
+// w[2^l + j], j = row >> (LOG_H - l); level 0 of the forward direction takes
+// plain residues (rsq / w[0] trick of kernel.cl:286-290).
+template <int S, bool INV>
+__device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int b, u32 o, const u32 * __restrict__ tw,
+	u32 p, u32 q, u32 rsq)
 {
-	constexpr int H = 1 << LOG_H;
+	u32 v[1 << S];
+	const u32 row0 = (o & ((1u << b) - 1)) | ((o >> b) << (b + S));
+	u32 * const base = colp + row0 * TW;
+	const u32 D = (u32)TW << b;
 #pragma unroll
-	for (int S = H / 2; S >= 1; S /= 2)
+	for (int g = 0; g < (1 << S); ++g) v[g] = base[g * D];
+	const u32 ohi = o >> b;
+#pragma unroll
+	for (int ss = 0; ss < S; ++ss)
 	{
-		const int m = H / (2 * S);
+		const int s = INV ? ss : (S - 1 - ss);
+		const int lvl = LOG_H - 1 - (b + s);
+		const u32 * __restrict__ twl = tw + ((1u << lvl) + (ohi << (S - 1 - s)));
 #pragma unroll
-		for (int j = 0; j < S; ++j)
+		for (int jh = 0; jh < (1 << (S - 1 - s)); ++jh)
 		{
-			const u32 wv = wi[S + j], wq = wv * q;
 #pragma unroll
-			for (int i = 0; i < m; ++i) inv_bfly(v[2 * m * j + i], v[2 * m * j + i + m], wv, wq, p);
+			for (int gl = 0; gl < (1 << s); ++gl)
+			{
+				const int g = (jh << (s + 1)) + gl;
+				if (INV)
+				{
+					const u32 wv = twl[jh];
+					inv_bfly(v[g], v[g + (1 << s)], wv, wv * q, p);
+				}
+				else if (lvl == 0)
+				{
+					const u32 w0 = tw[0];
+					const u32 a0 = mont_mul_c(v[g], rsq, rsq * q, p), t = mont_mul_c(v[g + (1 << s)], w0, w0 * q, p);
+					v[g] = add_mod(a0, t, p);
+					v[g + (1 << s)] = sub_mod(a0, t, p);
+				}
+				else
+				{
+					const u32 wv = twl[jh];
+					fwd_bfly(v[g], v[g + (1 << s)], wv, wv * q, p);
+				}
+			}
 		}
 	}
+#pragma unroll
+	for (int g = 0; g < (1 << S); ++g) base[g * D] = v[g];
 }
 
-template <int LOG_H>
-__device__ __forceinline__ void col_fwd(u32 (&v)[1 << LOG_H], const u32 * w, u32 p, u32 q, u32 rsq)
+// All LOG_H levels of the columns u in [u0, u0 + nu) of every prime, in place
+// in the tile; stages of 3 levels (the remainder first in the forward order).
+template <int LOG_H, int K, bool INV>
+__device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const u32 * twk, const TConst & c)
 {
 	constexpr int H = 1 << LOG_H;
+	constexpr int SR = (LOG_H % 3 == 0) ? 3 : LOG_H % 3;       // top stage (row bits LOG_H-SR..LOG_H-1)
+	constexpr int NST = 1 + (LOG_H - SR) / 3;
+	const int tid = (int)threadIdx.x, NT = (int)blockDim.x;
+#pragma unroll 1
+	for (int st = 0; st < NST; ++st)
 	{
-		const u32 w0 = w[0], w0q = w0 * q, rq = rsq * q;
-#pragma unroll
-		for (int i = 0; i < H / 2; ++i)
+		// forward: top stage first; inverse: bottom stage first
+		const int idx = INV ? (NST - 1 - st) : st;
+		const bool top = (idx == 0);
+		const int b = top ? (LOG_H - SR) : (LOG_H - SR - 3 * idx);
+		const int S = top ? SR : 3;
+		const int ntask = K * nu * (H >> S);
+		for (int task = tid; task < ntask; task += NT)
 		{
-			const u32 a = mont_mul_c(v[i], rsq, rq, p), t = mont_mul_c(v[i + H / 2], w0, w0q, p);
-			v[i] = add_mod(a, t, p);
-			v[i + H / 2] = sub_mod(a, t, p);
+			const int u = u0 + task % nu;
+			const int rest = task / nu;
+			const int o = rest % (H >> S), k = rest / (H >> S);
+			u32 * colp = tile + (k * H) * TW + u;
+			const u32 * tw = twk + k * H;
+			if (S == 3) col_step<3, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
+			else if (S == 2) col_step<2, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
+			else col_step<1, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
 		}
-	}
-#pragma unroll
-	for (int S = 2; S <= H / 2; S *= 2)
-	{
-		const int m = H / (2 * S);
-#pragma unroll
-		for (int j = 0; j < S; ++j)
-		{
-			const u32 wv = w[S + j], wq = wv * q;
-#pragma unroll
-			for (int i = 0; i < m; ++i) fwd_bfly(v[2 * m * j + i], v[2 * m * j + i + m], wv, wq, p);
-		}
+		__syncthreads();
 	}
 }
 
@@ -389,7 +461,7 @@ __device__ __forceinline__ i32 carry_phase2(const TConst & c, Big<K> f, const u3
 }
 
 template <int LOG_H, int K, int PCK>
-__global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TConst c)
+__global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, const TConst c)
 {
 	constexpr int H = 1 << LOG_H;
 	extern __shared__ __align__(16) u32 sm[];
@@ -403,7 +475,10 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 	const int nb = (int)gridDim.x, b = (int)blockIdx.x;
 	const u32 c0 = (u32)b * CC;
 	const bool single = (nb == 1);
-	const int E = (!J.transformed || single) ? 0 : ((b == 0) ? 8 : 4);
+	// predecessor columns: the 4 left of the CTA (the last 4 of the previous row
+	// for CTA 0); CTA 0 also takes the 4 before those when the mod R / mod Q
+	// decision needs the final top coefficient
+	const int E = (!J.transformed || single) ? 0 : ((b == 0 && J.lower != LOWER_NONE) ? 8 : 4);
 	const int WU = CC + E, ng = WU / 4;
 	const int tid = (int)threadIdx.x, NT = (int)blockDim.x;
 	const int lb = c.lbase;
@@ -430,17 +505,7 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 	if (J.transformed)
 	{
 		// ---- inverse column levels (all WU columns, K primes)
-		for (int task = tid; task < K * WU; task += NT)
-		{
-			const int k = task / WU, u = task % WU;
-			u32 v[H];
-#pragma unroll
-			for (int row = 0; row < H; ++row) v[row] = tile[(k * H + row) * TW + u];
-			col_inv<LOG_H>(v, twc + k * H, c.p[k], c.q[k]);
-#pragma unroll
-			for (int row = 0; row < H; ++row) tile[(k * H + row) * TW + u] = v[row];
-		}
-		__syncthreads();
+		col_transform<LOG_H, K, true>(tile, 0, WU, twc, c);
 
 		// ---- carry phase 1: per group, unsigned digits + carry-out
 		for (int idx = tid; idx < H * ng; idx += NT)
@@ -472,7 +537,8 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 				u32 rr[K];
 #pragma unroll
 				for (int k = 0; k < K; ++k) rr[k] = mont_mul(xv[k][j], c.norm[k], c.p[k], c.q[k]);
-				f = big_add<K>(f, big_mul_u32<K>(garner<K>(c, rr), J.a));
+				const Big<K> V = garner<K>(c, rr);
+				f = big_add<K>(f, (J.a == 1u) ? V : big_mul_u32<K>(V, J.a));
 				if (J.sub != nullptr)
 				{
 #pragma unroll
@@ -499,7 +565,7 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 			{
 				// CTA 0 re-derives the last coefficient of the register from its
 				// predecessor columns, for the mod R / mod Q decision
-				if (!(E == 8 && J.lower != LOWER_NONE)) continue;
+				if (E != 8) continue;
 				row = H - 1; u4 = 1; store = false;
 			}
 			else
@@ -508,9 +574,10 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 			}
 			int prow = row, pu4 = u4 - 1;
 			bool neg = false;
-			if (store && u4 == E / 4 && E != 4)
+			if (store && b == 0 && u4 == E / 4)
 			{
-				pu4 = (E == 8) ? 1 : (ng - 1);
+				// first group of a row: its predecessor ends the previous row
+				pu4 = (E == 0) ? (ng - 1) : (E / 4 - 1);
 				if (row > 0) prow = row - 1;
 				else { prow = H - 1; neg = (J.nega != 0); }
 			}
@@ -565,7 +632,9 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 		__syncthreads();
 	}
 
-	// ---- outputs: normal form and the first LA forward levels of the next product
+	// ---- outputs: normal form, then the first LA forward levels of the next
+	// product, computed in place (the second domain reloads the normal form
+	// from global memory)
 	if (J.out_norm != nullptr)
 	{
 		for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
@@ -574,20 +643,34 @@ __global__ void __launch_bounds__(256) k_colpass(const ColJobs jobs, const TCons
 			const uint4 val = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + E + 4 * u4);
 			*reinterpret_cast<uint4 *>(J.out_norm + (size_t)k * n + (size_t)row * R + c0 + 4 * u4) = val;
 		}
+		__syncthreads();
 	}
-	const int nd = (J.out_fwd[0] != nullptr ? 1 : 0) + (J.out_fwd[1] != nullptr ? 1 : 0);
-	for (int task = tid; task < nd * K * CC; task += NT)
+	bool reload = false;
+#pragma unroll 1
+	for (int dom = 0; dom < 2; ++dom)
 	{
-		int dom = task / (K * CC);
-		if (J.out_fwd[0] == nullptr) dom = 1;
-		const int k = (task / CC) % K, uc = task % CC;
-		u32 v[H];
-#pragma unroll
-		for (int row = 0; row < H; ++row) v[row] = tile[(k * H + row) * TW + E + uc];
-		col_fwd<LOG_H>(v, twc + (1 + dom) * K * H + k * H, c.p[k], c.q[k], c.rsq[k]);
-		u32 * const out = J.out_fwd[dom] + (size_t)k * n + c0 + uc;
-#pragma unroll
-		for (int row = 0; row < H; ++row) out[(size_t)row * R] = v[row];
+		u32 * const out = J.out_fwd[dom];
+		if (out == nullptr) continue;
+		if (reload)
+		{
+			__syncthreads();
+			const u32 * src = J.transformed ? J.out_norm : J.in;
+			for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
+			{
+				const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
+				*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + E + 4 * u4) =
+					*reinterpret_cast<const uint4 *>(src + (size_t)k * n + (size_t)row * R + c0 + 4 * u4);
+			}
+			__syncthreads();
+		}
+		col_transform<LOG_H, K, false>(tile, E, CC, twc + (1 + dom) * K * H, c);
+		for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
+		{
+			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
+			*reinterpret_cast<uint4 *>(out + (size_t)k * n + (size_t)row * R + c0 + 4 * u4) =
+				*reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + E + 4 * u4);
+		}
+		reload = true;
 	}
 }
 
@@ -613,7 +696,7 @@ template <int LOG_R>
 static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s)
 {
 	const u32 R = 1u << LOG_R;
-	const size_t smem = sizeof(u32) * (R + R / 32);
+	const size_t smem = sizeof(u32) * (R + R / 16);
 	static bool attr = false;
 	if (!attr)
 	{
@@ -622,7 +705,7 @@ static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs
 		attr = true;
 	}
 	const dim3 grid((unsigned)(c.K * g.H), (unsigned)njobs);
-	k_rowpass<LOG_R><<<grid, R / 32, smem, s>>>(jobs, c);
+	k_rowpass<LOG_R><<<grid, RowCfg<LOG_R>::NT, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
 
@@ -656,7 +739,7 @@ static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs
 		attr = true;
 	}
 	const dim3 grid(g.R / CC, (unsigned)njobs);
-	k_colpass<LOG_H, K, PCK><<<grid, 256, smem, s>>>(jobs, c);
+	k_colpass<LOG_H, K, PCK><<<grid, COL_THREADS, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
 
