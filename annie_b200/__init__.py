@@ -42,8 +42,31 @@ class Params(C.Structure):
         return (self.K, self.pck, self.ln, self.lbase)
 
 
+class PrpOptions(C.Structure):
+    _fields_ = [("euler", C.c_int), ("base", C.c_int32), ("device", C.c_int), ("gl_check_blocks", C.c_int),
+                ("inject_iteration", C.c_int64), ("inject_word", C.c_uint32), ("checkpoint_path", C.c_char_p),
+                ("checkpoint_seconds", C.c_double), ("verbose", C.c_int)]
+
+
+class PrpResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("decided_early", C.c_int), ("is_prp", C.c_int), ("res64", C.c_uint64),
+                ("base", C.c_int32), ("K", C.c_int), ("pck", C.c_int), ("ln", C.c_int), ("lbase", C.c_int),
+                ("gl_block", C.c_int), ("squarings", C.c_int64), ("gl_checks", C.c_int), ("gl_failures", C.c_int),
+                ("rollbacks", C.c_int), ("resumed", C.c_int), ("seconds", C.c_double), ("message", C.c_char * 256)]
+
+    def asdict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["message"] = self.message.decode(errors="replace")
+        return d
+
+
+class RunnerOptions(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots_per_class", C.c_int), ("chunk", C.c_int)]
+
+
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
 _lib = None
 
 # (name, argtypes, restype) of every exported symbol of include/annie_b200.h
@@ -75,6 +98,28 @@ ABI = [
     ("ab_profile_square", [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)], C.c_int),
     ("ab_flush_l2", [C.c_void_p, C.c_size_t], C.c_int),
     ("ab_square_mul_noalloc", [C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
+    ("ab_prp_options_default", [C.POINTER(PrpOptions)], None),
+    ("ab_prp_check", [_u64p, C.c_size_t, C.POINTER(PrpOptions), C.POINTER(PrpResult)], C.c_int),
+    ("ab_prp_quit", [], None),
+    ("ab_prp_reset_quit", [], None),
+    ("ab_batch_slot_bytes", [C.POINTER(Params)], C.c_size_t),
+    ("ab_batch_create", [C.c_int, C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    ("ab_batch_destroy", [C.c_void_p], None),
+    ("ab_batch_load", [C.c_void_p, C.c_int, _u64p, C.c_size_t, C.c_int32, C.POINTER(C.c_int)], C.c_int),
+    ("ab_batch_slot", [C.c_void_p, C.c_int], C.c_void_p),
+    ("ab_batch_release", [C.c_void_p, C.c_int], C.c_int),
+    ("ab_batch_steps", [C.c_void_p, C.c_int, _u32p, _u8p], C.c_int),
+    ("ab_batch_gl_mul", [C.c_void_p, C.c_int], C.c_int),
+    ("ab_batch_set_geometry", [C.c_void_p, C.c_int], C.c_int),
+    ("ab_batch_synchronize", [C.c_void_p], C.c_int),
+    ("ab_batch_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
+    ("ab_runner_options_default", [C.POINTER(RunnerOptions)], None),
+    ("ab_runner_create", [C.POINTER(RunnerOptions), C.POINTER(C.c_void_p)], C.c_int),
+    ("ab_runner_destroy", [C.c_void_p], None),
+    ("ab_runner_submit", [C.c_void_p, _u64p, C.c_size_t, C.c_int, C.c_int32, C.c_uint64], C.c_int),
+    ("ab_runner_advance", [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    ("ab_runner_poll", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(PrpResult)], C.c_int),
+    ("ab_runner_stats", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_int)], C.c_int),
     ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
     ("ab_diag_product", [C.c_void_p, C.c_int, _u32p, _u32p, C.c_uint32, _u32p, C.c_int, _u32p], C.c_int),
 ]
@@ -121,6 +166,23 @@ def probe(N, a, forced=None):
     fp = None if forced is None else C.byref(Params(*forced))
     _check(lib().ab_probe(limbs.ctypes.data_as(_u64p), len(limbs), a, fp, C.byref(out), C.byref(failed)))
     return out.astuple(), bool(failed.value)
+
+
+def prp_check(N, euler=False, base=0, device=0, gl_check_blocks=0, inject_iteration=-1, inject_word=0,
+              checkpoint_path=None, checkpoint_seconds=600.0):
+    """Full probable-prime test of N (the reference's annie::check, src/annie.h:217-430)
+    with optional periodic Gerbicz-Li checks, rollback and fault injection.  Returns a dict."""
+    L = lib()
+    o = PrpOptions()
+    L.ab_prp_options_default(C.byref(o))
+    o.euler, o.base, o.device, o.gl_check_blocks = int(euler), base, device, gl_check_blocks
+    o.inject_iteration, o.inject_word = inject_iteration, inject_word
+    o.checkpoint_path = None if checkpoint_path is None else checkpoint_path.encode()
+    o.checkpoint_seconds = checkpoint_seconds
+    r = PrpResult()
+    limbs = int_to_limbs(N)
+    L.ab_prp_check(limbs.ctypes.data_as(_u64p), len(limbs), C.byref(o), C.byref(r))
+    return r.asdict()
 
 
 class Transform:
@@ -284,3 +346,126 @@ class Transform:
                                       None if sba is None else sba.ctypes.data_as(_u32p), lower_mode,
                                       out.ctypes.data_as(_u32p)))
         return out
+
+
+class SlotView(Transform):
+    """A batch slot used through the transform interface (owned by its Batch)."""
+
+    def __init__(self, batch, slot, handle):
+        self.N, self.a = batch.Ns[slot], batch.bases[slot]
+        self.L = batch.L
+        self.h = C.c_void_p(handle)
+        info = Params()
+        _check(self.L.ab_info(self.h, C.byref(info)))
+        self.K, self.pck, self.ln, self.lbase = info.astuple()
+        self.n = 1 << self.ln
+        self._cap = len(int_to_limbs(self.N)) + 2
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Size class (K, pck, ln) of `capacity` slots squared together (captured CUDA graph)."""
+
+    def __init__(self, cls, capacity, max_steps=64, device=0):
+        self.L = lib()
+        self.cls = Params(*cls)
+        self.capacity, self.max_steps = capacity, max_steps
+        h = C.c_void_p()
+        _check(self.L.ab_batch_create(device, C.byref(self.cls), capacity, max_steps, C.byref(h)))
+        self.h = h
+        self.Ns = [None] * capacity
+        self.bases = [None] * capacity
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ab_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, slot, N, a):
+        limbs = int_to_limbs(N)
+        failed = C.c_int()
+        _check(self.L.ab_batch_load(self.h, slot, limbs.ctypes.data_as(_u64p), len(limbs), a, C.byref(failed)))
+        self.Ns[slot], self.bases[slot] = N, a
+        return bool(failed.value)
+
+    def slot(self, slot):
+        hv = self.L.ab_batch_slot(self.h, slot)
+        return None if not hv else SlotView(self, slot, hv)
+
+    def release(self, slot):
+        _check(self.L.ab_batch_release(self.h, slot))
+        self.Ns[slot] = None
+
+    def steps(self, mult, snap=None):
+        """mult: array [steps, capacity] of multipliers (0 = idle); snap: same shape, nonzero = keep Reg0."""
+        m = np.ascontiguousarray(mult, dtype=np.uint32)
+        s = None if snap is None else np.ascontiguousarray(snap, dtype=np.uint8)
+        _check(self.L.ab_batch_steps(self.h, m.shape[0], m.ctypes.data_as(_u32p), None if s is None else s.ctypes.data_as(_u8p)))
+
+    def gl_mul(self, slot):
+        _check(self.L.ab_batch_gl_mul(self.h, slot))
+
+    def set_geometry(self, lb):
+        _check(self.L.ab_batch_set_geometry(self.h, lb))
+
+    def synchronize(self):
+        _check(self.L.ab_batch_synchronize(self.h))
+
+    def launch_count(self):
+        c = C.c_uint64()
+        _check(self.L.ab_batch_launch_count(self.h, C.byref(c)))
+        return c.value
+
+
+class Runner:
+    """Continuous-batching PRP runner: submit tests, advance, poll results."""
+
+    def __init__(self, device=0, hbm_budget_bytes=32 << 30, max_slots_per_class=256, chunk=64):
+        self.L = lib()
+        o = RunnerOptions()
+        self.L.ab_runner_options_default(C.byref(o))
+        o.device, o.hbm_budget_bytes, o.max_slots_per_class, o.chunk = device, hbm_budget_bytes, max_slots_per_class, chunk
+        h = C.c_void_p()
+        _check(self.L.ab_runner_create(C.byref(o), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ab_runner_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, N, euler=False, base=0, tag=0):
+        limbs = int_to_limbs(N)
+        _check(self.L.ab_runner_submit(self.h, limbs.ctypes.data_as(_u64p), len(limbs), int(euler), base, tag))
+
+    def advance(self):
+        a, q = C.c_int(), C.c_int()
+        _check(self.L.ab_runner_advance(self.h, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def poll(self):
+        tag = C.c_uint64()
+        r = PrpResult()
+        out = []
+        while self.L.ab_runner_poll(self.h, C.byref(tag), C.byref(r)):
+            out.append((tag.value, r.asdict()))
+        return out
+
+    def stats(self):
+        s, l, b = C.c_uint64(), C.c_uint64(), C.c_int()
+        _check(self.L.ab_runner_stats(self.h, C.byref(s), C.byref(l), C.byref(b)))
+        return {"squarings": s.value, "launches": l.value, "batches": b.value}

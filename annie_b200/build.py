@@ -19,13 +19,18 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
+HOST = os.path.join(HERE, "host")
+
+
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return (sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")) +
+            sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp")))
 
 
 def deps():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)) + [
-        os.path.join(HERE, "..", "include", "annie_b200.h"), os.path.join(HERE, "gmp", "gmp.h")]
+    inc = os.path.join(HERE, "..", "include")
+    return (sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)) + sorted(os.path.join(HOST, f) for f in os.listdir(HOST)) +
+            sorted(os.path.join(inc, f) for f in os.listdir(inc)) + [os.path.join(HERE, "gmp", "gmp.h")])
 
 
 def up_to_date():
@@ -42,9 +47,9 @@ def build(force=False, ptxas_verbose=False, jobs=None):
     objs = []
     procs = []
     for src in sources():
-        obj = os.path.join(LIBDIR, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(LIBDIR, os.path.basename(src).rsplit(".", 1)[0] + ".o")
         cmd = [NVCC, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-c",
-               "-I" + os.path.join(HERE, "gmp"), "-I" + CSRC, src, "-o", obj]
+               "-I" + os.path.join(HERE, "gmp"), "-I" + CSRC, "-I" + HOST, src, "-o", obj]
         if ptxas_verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

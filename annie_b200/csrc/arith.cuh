@@ -65,6 +65,15 @@ struct TConst
 	int LA, LB;                 // column levels, row levels
 };
 
+// Digit constants of one candidate (the digit size may differ between the
+// candidates of a batch that share K and the NTT length).
+struct CandConst
+{
+	int lbase;
+	u32 rbase[AB_MAXK];         // Montgomery form of 2^lbase
+	u32 rbase_pck[AB_MAXK];     // 2^(pck*lbase) mod p
+};
+
 // ---------------------------------------------------------------- big ints
 template <int K>
 struct Big
@@ -278,18 +287,19 @@ __device__ __forceinline__ Big<K> add_digits(const Big<K> & f, int lb, const u32
 // [0, base)) for each prime: Horner in the plain domain, top digit first
 // (same value as encode() in ocl/kernel.cl:1474).
 template <int K, int PCK>
-__device__ __forceinline__ void encode_digits(const TConst & c, i32 top, const u32 (&d)[PCK], u32 (&x)[K])
+__device__ __forceinline__ void encode_digits(const TConst & c, const u32 * rbase, i32 top, const u32 (&d)[PCK], u32 (&x)[K])
 {
 #pragma unroll
 	for (int k = 0; k < K; ++k)
 	{
 		const u32 p = c.p[k];
 		u32 v = set_i32(top, p);
+		const u32 rb = rbase[k];
 #pragma unroll
 		for (int l = PCK - 2; l >= 0; --l)
 		{
 			// v = v * base + d_l  (base plain: mont(v, base*2^32) = v * base)
-			v = mont_mul(v, c.rbase[k], p, c.q[k]);
+			v = mont_mul(v, rb, p, c.q[k]);
 			v = add_mod(v, d[l], p);
 		}
 		x[k] = v;

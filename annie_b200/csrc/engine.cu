@@ -156,7 +156,7 @@ bool compute_R_Ninv(const mpz_t N, const ab_params & p, mpz_t R, mpz_t Ninv, mpz
 // ============================================================ the engine
 struct ab_transform
 {
-	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, NQ, NIR, OPQ, OPR, AQ0, AQ1, AR0, AR1, TMP, WR, WQ, NBUF };
+	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, NQ, NIR, OPQ, OPR, AQ0, AQ1, AR0, AR1, TMP, SNAP, WR, WQ, NBUF };
 
 	int device = 0;
 	cudaStream_t st = nullptr;
@@ -177,10 +177,14 @@ struct ab_transform
 	size_t prof_used = 0;
 	void * flush_buf = nullptr;
 
-	u32 * b(int i) const { return dmem + (size_t)i * prm.K * n; }
+	u32 * bufp[NBUF] = {};   // device buffers (a batch slot view points into its batch)
+	bool view = false;       // true: memory and streams belong to a batch
+
+	u32 * b(int i) const { return bufp[i]; }
 
 	~ab_transform()
 	{
+		if (view) { mpz_clears(N, factor, nullptr); return; }
 		for (cudaEvent_t e : prof) cudaEventDestroy(e);
 		if (flush_buf) cudaFree(flush_buf);
 		if (dmem) cudaFree(dmem);
@@ -307,7 +311,7 @@ struct ab_transform
 	}
 	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp = nullptr) const
 	{
-		RowJob j; j.x = x; j.xp = xp; j.w = w; j.mode = mode; return j;
+		RowJob j; std::memset(&j, 0, sizeof(j)); j.x = x; j.xp = xp; j.w = w; j.mode = mode; return j;
 	}
 	ColJob cj_norm(const u32 * in) const
 	{
@@ -428,11 +432,17 @@ struct ab_transform
 		decode(host.data(), z);
 	}
 
-	void init(const mpz_t Nin, int32_t a, int dev, const ab_params * forced)
+	// host part of the set-up: parameters, geometry, R, N^-1 mod R, constants,
+	// and the register words of N, N^-1 and the MMGW form of 1
+	struct Prepared
+	{
+		std::vector<u32> wN, wNinv, wOne;
+	};
+
+	void prepare(const mpz_t Nin, int32_t a, const ab_params * forced, Prepared & pp)
 	{
 		mpz_inits(N, factor, nullptr);
 		mpz_set(N, Nin);
-		device = dev;
 		prm = forced ? *forced : select_params(N, a);
 		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31)
 			throw ab_error(AB_E_ARG, "invalid transform parameters");
@@ -441,6 +451,35 @@ struct ab_transform
 		mpz_t R, Ninv; mpz_inits(R, Ninv, nullptr);
 		if (!compute_R_Ninv(N, prm, R, Ninv, factor)) { failed = true; mpz_clears(R, Ninv, nullptr); return; }
 		build_consts();
+		const size_t words = (size_t)prm.K * n;
+		pp.wN.resize(words); pp.wNinv.resize(words); pp.wOne.resize(words);
+		encode(N, pp.wN.data());
+		encode(Ninv, pp.wNinv.data());
+		// MMGW form of 1 is R/2 mod N (transformGPU.h:743-747)
+		mpz_mod(Ninv, R, N);
+		if (mpz_odd_p(Ninv)) mpz_add(Ninv, Ninv, N);
+		mpz_fdiv_q_2exp(Ninv, Ninv, 1);
+		encode(Ninv, pp.wOne.data());
+		mpz_clears(R, Ninv, nullptr);
+	}
+
+	// device part: forward transforms of N (domain Q) and N^-1 (domain R), and 1
+	void setup_device(const Prepared & pp)
+	{
+		upload(TMP, pp.wN.data());
+		full_forward(b(TMP), b(NQ), nullptr);
+		upload(TMP, pp.wNinv.data());
+		full_forward(b(TMP), nullptr, b(NIR));
+		upload(ONE, pp.wOne.data());
+		CK(cudaStreamSynchronize(st));
+	}
+
+	void init(const mpz_t Nin, int32_t a, int dev, const ab_params * forced)
+	{
+		device = dev;
+		Prepared pp;
+		prepare(Nin, a, forced, pp);
+		if (failed) return;
 
 		CK(cudaSetDevice(device));
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -450,24 +489,107 @@ struct ab_transform
 		CK(cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming));
 		CK(cudaMalloc(&dmem, (size_t)NBUF * prm.K * n * 4));
 		CK(cudaMemsetAsync(dmem, 0, (size_t)NBUF * prm.K * n * 4, st));
+		for (int i = 0; i < NBUF; ++i) bufp[i] = dmem + (size_t)i * prm.K * n;
 
 		host.assign((size_t)prm.K * n, 0);
 		std::vector<u32> wr((size_t)prm.K * n), wq((size_t)prm.K * n);
 		for (int k = 0; k < prm.K; ++k) { make_roots(&wr[(size_t)k * n], prm.ln, k, false); make_roots(&wq[(size_t)k * n], prm.ln, k, true); }
 		upload(WR, wr.data()); upload(WQ, wq.data());
+		setup_device(pp);
+	}
+};
 
-		encode(N, host.data()); upload(TMP, host.data());
-		full_forward(b(TMP), b(NQ), nullptr);
-		CK(cudaStreamSynchronize(st));
-		encode(Ninv, host.data()); upload(TMP, host.data());
-		full_forward(b(TMP), nullptr, b(NIR));
-		CK(cudaStreamSynchronize(st));
-		// MMGW form of 1 is R/2 mod N (transformGPU.h:743-747)
-		mpz_mod(Ninv, R, N);
-		if (mpz_odd_p(Ninv)) mpz_add(Ninv, Ninv, N);
-		mpz_fdiv_q_2exp(Ninv, Ninv, 1);
-		encode(Ninv, host.data()); upload(ONE, host.data());
-		mpz_clears(R, Ninv, nullptr);
+// ============================================================ batches
+// A size class (K, pck, ln) of `cap` candidates with stacked buffers: buffer
+// type i of slot s is at base[i] + s * words.  Each loaded slot is exposed as
+// an ab_transform view (set1 / copy / mul / get work unchanged on it); the
+// squarings of all slots run together (grid.z = slot) from a captured CUDA
+// graph whose per-step, per-slot multipliers are uploaded before each launch.
+struct ab_batch
+{
+	int device = 0;
+	cudaStream_t st = nullptr;
+	ab_params cls{};
+	Geometry geo{};
+	TConst tc{};
+	size_t n = 0, words = 0;
+	int cap = 0, max_steps = 0;
+	u32 * mem = nullptr;
+	u32 * base[ab_transform::NBUF] = {};
+	CandConst * d_cand = nullptr;
+	std::vector<CandConst> h_cand;
+	u32 * d_ctrl = nullptr;            // per step: mult[cap] | act[cap] | snap[cap]
+	std::vector<u32> h_ctrl;
+	std::vector<ab_transform *> views;
+	cudaGraphExec_t gexec = nullptr;
+	int g_steps = 0;
+	uint64_t launches = 0;
+
+	~ab_batch()
+	{
+		for (ab_transform * v : views) delete v;
+		if (gexec) cudaGraphExecDestroy(gexec);
+		if (mem) cudaFree(mem);
+		if (d_cand) cudaFree(d_cand);
+		if (d_ctrl) cudaFree(d_ctrl);
+		if (st) cudaStreamDestroy(st);
+	}
+
+	u32 * ctrl(int step, int part) const { return d_ctrl + ((size_t)step * 3 + part) * cap; }
+
+	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
+	{
+		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st, cap));
+	}
+	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
+	{
+		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, cap));
+	}
+	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp, const u32 * act) const
+	{
+		RowJob j; std::memset(&j, 0, sizeof(j));
+		j.x = x; j.xp = xp; j.w = w; j.mode = mode; j.stride = words; j.active = act;
+		return j;
+	}
+	ColJob cj(const u32 * in, bool tr, const u32 * w_in, const u32 * mult, int nega, const u32 * sub, int lower) const
+	{
+		ColJob j; std::memset(&j, 0, sizeof(j));
+		j.in = in; j.transformed = tr ? 1 : 0; j.w_in = w_in; j.a = 1; j.mult = mult; j.nega = nega; j.sub = sub;
+		j.lower = lower; j.stride = words; j.cand = d_cand;
+		return j;
+	}
+
+	// squareMMGW (transformGPU.h:556-568) for every slot, `steps` times
+	void record_steps(int steps)
+	{
+		using T = ab_transform;
+		u32 * const aq0 = base[T::AQ0], * const ar0 = base[T::AR0], * const aq1 = base[T::AQ1], * const ar1 = base[T::AR1];
+		const u32 * wq = base[T::WQ], * wr = base[T::WR];
+		{
+			ColJob j = cj(base[T::REG0], false, nullptr, ctrl(0, 1), 0, nullptr, LOWER_NONE);
+			j.out_fwd[0] = aq0; j.w_out[0] = wq; j.out_fwd[1] = ar0; j.w_out[1] = wr;
+			cols(j);
+		}
+		for (int s = 0; s < steps; ++s)
+		{
+			const u32 * mult = ctrl(s, 0), * act = ctrl(s, 1), * snap = ctrl(s, 2);
+			RowJob rq = rj(aq0, ROW_SQUARE, wq, nullptr, act), rr = rj(ar0, ROW_SQUARE, wr, nullptr, act);
+			rows(rq, &rr);
+			ColJob jq = cj(aq0, true, wq, mult, 1, nullptr, LOWER_NONE); jq.out_norm = base[T::TQ];
+			ColJob jr = cj(ar0, true, wr, mult, 0, nullptr, LOWER_NONE); jr.out_fwd[1] = ar1; jr.w_out[1] = wr;
+			cols(jq, &jr);
+			rows(rj(ar1, ROW_MUL, wr, base[T::NIR], act));
+			ColJob j1 = cj(ar1, true, wr, act, 0, nullptr, LOWER_R_ADD2); j1.out_fwd[0] = aq1; j1.w_out[0] = wq;
+			cols(j1);
+			rows(rj(aq1, ROW_MUL, wq, base[T::NQ], act));
+			ColJob j2 = cj(aq1, true, wq, act, 1, base[T::TQ], LOWER_Q);
+			j2.out_norm = base[T::REG0];
+			j2.out_fwd[0] = aq0; j2.w_out[0] = wq; j2.out_fwd[1] = ar0; j2.w_out[1] = wr;
+			j2.out_snap = base[T::SNAP]; j2.snap_flag = snap;
+			cols(j2);
+		}
 	}
 };
 
@@ -821,6 +943,186 @@ int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uin
 		h->download(T::TMP, out, (size_t)h->prm.K);
 		h->prefwd = false;
 	});
+}
+
+
+size_t ab_batch_slot_bytes(const ab_params * cls)
+{
+	if (cls == nullptr) return 0;
+	return (size_t)(ab_transform::WR) * cls->K * ((size_t)1 << cls->ln) * 4;
+}
+
+int ab_batch_create(int device, const ab_params * cls, int capacity, int max_steps, ab_batch ** out)
+{
+	if (out) *out = nullptr;
+	ab_batch * b = nullptr;
+	const int rc = guarded([&] {
+		if (cls == nullptr || out == nullptr || capacity < 1 || max_steps < 1) throw ab_error(AB_E_ARG, "bad arguments");
+		if (cls->K < 2 || cls->K > 5 || (size_t)cls->pck != get_s((size_t)cls->K)) throw ab_error(AB_E_ARG, "invalid size class");
+		b = new ab_batch();
+		b->device = device; b->cls = *cls; b->cap = capacity; b->max_steps = max_steps;
+		if (!make_geometry(cls->ln, 0, b->geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length not supported");
+		b->n = (size_t)1 << cls->ln; b->words = (size_t)cls->K * b->n;
+		CK(cudaSetDevice(device));
+		CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+		const size_t per = (size_t)ab_transform::WR;          // per-slot buffer types
+		CK(cudaMalloc(&b->mem, (per * capacity + 2) * b->words * 4));
+		CK(cudaMemsetAsync(b->mem, 0, (per * capacity + 2) * b->words * 4, b->st));
+		for (size_t i = 0; i < per; ++i) b->base[i] = b->mem + i * capacity * b->words;
+		b->base[ab_transform::WR] = b->mem + per * capacity * b->words;
+		b->base[ab_transform::WQ] = b->base[ab_transform::WR] + b->words;
+		std::vector<u32> wr(b->words), wq(b->words);
+		for (int k = 0; k < cls->K; ++k) { make_roots(&wr[(size_t)k * b->n], cls->ln, k, false); make_roots(&wq[(size_t)k * b->n], cls->ln, k, true); }
+		CK(cudaMemcpyAsync(b->base[ab_transform::WR], wr.data(), b->words * 4, cudaMemcpyHostToDevice, b->st));
+		CK(cudaMemcpyAsync(b->base[ab_transform::WQ], wq.data(), b->words * 4, cudaMemcpyHostToDevice, b->st));
+		CK(cudaMalloc(&b->d_cand, sizeof(CandConst) * capacity));
+		b->h_cand.assign(capacity, CandConst{});
+		for (auto & c : b->h_cand) c.lbase = 2;
+		CK(cudaMemcpyAsync(b->d_cand, b->h_cand.data(), sizeof(CandConst) * capacity, cudaMemcpyHostToDevice, b->st));
+		CK(cudaMalloc(&b->d_ctrl, (size_t)3 * max_steps * capacity * 4));
+		CK(cudaMemsetAsync(b->d_ctrl, 0, (size_t)3 * max_steps * capacity * 4, b->st));
+		b->h_ctrl.assign((size_t)3 * max_steps * capacity, 0);
+		b->views.assign(capacity, nullptr);
+		// TConst of the class (digit constants come from d_cand)
+		ab_transform probe_t;
+		probe_t.prm = *cls; probe_t.prm.lbase = 17; probe_t.n = b->n; probe_t.geo = b->geo;
+		probe_t.build_consts();
+		b->tc = probe_t.tc;
+		mpz_inits(probe_t.N, probe_t.factor, nullptr);
+		probe_t.view = true;
+		// kernel attributes before any capture
+		RowJobs rjs{}; ColJobs cjs{};
+		CK(launch_rowpass(b->geo, b->tc, rjs, 1, b->st, 0));
+		CK(launch_colpass(b->geo, b->tc, cjs, 1, b->st, 0));
+		CK(cudaStreamSynchronize(b->st));
+	});
+	if (rc != AB_OK) { delete b; return rc; }
+	*out = b;
+	return AB_OK;
+}
+
+void ab_batch_destroy(ab_batch * b) { delete b; }
+
+int ab_batch_load(ab_batch * b, int slot, const uint64_t * Nl, size_t nlimbs, int32_t a, int * init_failed)
+{
+	return guarded([&] {
+		if (b == nullptr || slot < 0 || slot >= b->cap || Nl == nullptr || nlimbs == 0 || a < 1) throw ab_error(AB_E_ARG, "bad arguments");
+		delete b->views[slot];
+		b->views[slot] = nullptr;
+		ab_transform * v = new ab_transform();
+		try
+		{
+			mpz_t N; mpz_init(N); mpz_from_limbs(N, Nl, nlimbs);
+			ab_transform::Prepared pp;
+			v->view = true;
+			v->prepare(N, a, nullptr, pp);
+			mpz_clear(N);
+			if (!v->failed && (v->prm.K != b->cls.K || v->prm.pck != b->cls.pck || v->prm.ln != b->cls.ln))
+				throw ab_error(AB_E_ARG, "N does not belong to this size class");
+			if (init_failed) *init_failed = v->failed ? 1 : 0;
+			v->device = b->device; v->st = b->st; v->overlap = false; v->geo = b->geo;
+			for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
+			v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
+			v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
+			if (!v->failed)
+			{
+				v->host.assign(b->words, 0);
+				v->setup_device(pp);
+				CandConst & c = b->h_cand[slot];
+				c.lbase = v->prm.lbase;
+				for (int k = 0; k < AB_MAXK; ++k) { c.rbase[k] = v->tc.rbase[k]; c.rbase_pck[k] = v->tc.rbase_pck[k]; }
+				CK(cudaMemcpyAsync(b->d_cand + slot, &c, sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
+				CK(cudaStreamSynchronize(b->st));
+			}
+		}
+		catch (...) { delete v; throw; }
+		b->views[slot] = v;
+	});
+}
+
+ab_transform * ab_batch_slot(ab_batch * b, int slot)
+{
+	if (b == nullptr || slot < 0 || slot >= b->cap) return nullptr;
+	return b->views[slot];
+}
+
+int ab_batch_release(ab_batch * b, int slot)
+{
+	return guarded([&] {
+		if (b == nullptr || slot < 0 || slot >= b->cap) throw ab_error(AB_E_ARG, "bad arguments");
+		delete b->views[slot];
+		b->views[slot] = nullptr;
+	});
+}
+
+int ab_batch_gl_mul(ab_batch * b, int slot)
+{
+	return guarded([&] {
+		if (b == nullptr || slot < 0 || slot >= b->cap || b->views[slot] == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		need_ready(b->views[slot]);
+		b->views[slot]->mul(ab_transform::REG1, ab_transform::SNAP);
+	});
+}
+
+int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t * snap)
+{
+	return guarded([&] {
+		if (b == nullptr || mult == nullptr || steps < 1 || steps > b->max_steps) throw ab_error(AB_E_ARG, "bad arguments");
+		const int cap = b->cap;
+		for (int s = 0; s < steps; ++s)
+			for (int c = 0; c < cap; ++c)
+			{
+				const bool live = b->views[c] != nullptr && !b->views[c]->failed;
+				const u32 m = live ? mult[(size_t)s * cap + c] : 0u;
+				b->h_ctrl[((size_t)s * 3 + 0) * cap + c] = m;
+				b->h_ctrl[((size_t)s * 3 + 1) * cap + c] = (m != 0u) ? 1u : 0u;
+				b->h_ctrl[((size_t)s * 3 + 2) * cap + c] = (snap != nullptr && m != 0u && snap[(size_t)s * cap + c]) ? 1u : 0u;
+			}
+		CK(cudaMemcpyAsync(b->d_ctrl, b->h_ctrl.data(), (size_t)3 * steps * cap * 4, cudaMemcpyHostToDevice, b->st));
+		if (b->gexec == nullptr || b->g_steps != steps)
+		{
+			if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+			cudaGraph_t g = nullptr;
+			CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+			try { b->record_steps(steps); }
+			catch (...) { cudaStreamEndCapture(b->st, &g); if (g) cudaGraphDestroy(g); throw; }
+			CK(cudaStreamEndCapture(b->st, &g));
+			const cudaError_t e = cudaGraphInstantiate(&b->gexec, g, 0);
+			cudaGraphDestroy(g);
+			CK(e);
+			b->g_steps = steps;
+		}
+		CK(cudaGraphLaunch(b->gexec, b->st));
+		b->launches += 1 + 6 * (uint64_t)steps;       // kernels of the graph
+		for (ab_transform * v : b->views) if (v) v->prefwd = false;
+	});
+}
+
+int ab_batch_set_geometry(ab_batch * b, int lb)
+{
+	return guarded([&] {
+		if (b == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		Geometry g;
+		if (!make_geometry(b->cls.ln, lb, g)) throw ab_error(AB_E_ARG, "geometry not available for this length");
+		CK(cudaStreamSynchronize(b->st));
+		b->geo = g;
+		b->tc.R = g.R; b->tc.H = g.H; b->tc.LA = g.LA; b->tc.LB = g.LB;
+		for (ab_transform * v : b->views) if (v) { v->geo = g; v->tc.R = g.R; v->tc.H = g.H; v->tc.LA = g.LA; v->tc.LB = g.LB; }
+		RowJobs rjs{}; ColJobs cjs{};
+		CK(launch_rowpass(b->geo, b->tc, rjs, 1, b->st, 0));
+		CK(launch_colpass(b->geo, b->tc, cjs, 1, b->st, 0));
+		if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+	});
+}
+
+int ab_batch_synchronize(ab_batch * b)
+{
+	return guarded([&] { if (b == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); CK(cudaStreamSynchronize(b->st)); });
+}
+
+int ab_batch_launch_count(const ab_batch * b, uint64_t * count)
+{
+	return guarded([&] { if (b == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); *count = b->launches; });
 }
 
 }

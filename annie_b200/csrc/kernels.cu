@@ -221,12 +221,15 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 3) k_rowpass(const RowJobs 
 	extern __shared__ __align__(16) u32 sm[];
 
 	const RowJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
+	const u32 cand = blockIdx.z;
+	if (J.active != nullptr && J.active[cand] == 0u) return;
+	const size_t cofs = (size_t)cand * J.stride;
 	const u32 k = blockIdx.x / c.H, r = blockIdx.x - k * c.H;
 	const u32 p = c.p[k], q = c.q[k];
-	u32 * __restrict__ x = J.x + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
+	u32 * __restrict__ x = J.x + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
 	const u32 * __restrict__ w = J.w + (size_t)k * c.n;
 	const u32 * __restrict__ wi = w + (c.n >> 1);
-	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
+	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
 	const u32 Hr = c.H + r;
 	const u32 tid = threadIdx.x;
 	u32 v[RP_EPT];
@@ -418,9 +421,8 @@ __device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const 
 // group's unsigned digits; writes the balanced re-encoded residues and returns
 // the top sub-digit of the last coefficient (kernel.cl:1582-1613).
 template <int K, int PCK>
-__device__ __forceinline__ i32 carry_phase2(const TConst & c, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
+__device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 * rbase, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
 {
-	const int lb = c.lbase;
 	const i32 base = (i32)(1u << lb);
 #pragma unroll
 	for (int j = 0; j < 3; ++j)
@@ -430,7 +432,7 @@ __device__ __forceinline__ i32 carry_phase2(const TConst & c, Big<K> f, const u3
 		extract_shift<K, PCK>(f, lb, e);
 		i32 top = (i32)e[PCK - 1];
 		if (top >= base / 2) { top -= base; f = big_add_u32<K>(f, 1u); }
-		encode_digits<K, PCK>(c, top, e, res[j]);
+		encode_digits<K, PCK>(c, rbase, top, e, res[j]);
 	}
 	f = add_digits<K, PCK>(f, lb, d[3]);
 	const u32 bm = (u32)base - 1;
@@ -456,7 +458,7 @@ __device__ __forceinline__ i32 carry_phase2(const TConst & c, Big<K> f, const u3
 		e[2 % PCK] = (u32)r23 & bm;
 		top = (i32)(r23 >> lb);
 	}
-	encode_digits<K, PCK>(c, top, e, res[3]);
+	encode_digits<K, PCK>(c, rbase, top, e, res[3]);
 	return top;
 }
 
@@ -469,8 +471,21 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	u32 * const cw = tile + K * H * TW;          // [H][TW/4][K] carry-out words
 	u32 * const twc = cw + H * (TW / 4) * K;     // [3][K][H] column twiddles
 	__shared__ int decision;
+	__shared__ CandConst cc;
 
-	const ColJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
+	ColJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
+	const u32 cand = blockIdx.z;
+	const u32 amul = (J.mult != nullptr) ? J.mult[cand] : J.a;
+	if (amul == 0u) return;                       // inactive batch slot
+	{
+		const size_t cofs = (size_t)cand * J.stride;
+		J.in += cofs;
+		if (J.sub) J.sub += cofs;
+		if (J.out_norm) J.out_norm += cofs;
+		if (J.out_fwd[0]) J.out_fwd[0] += cofs;
+		if (J.out_fwd[1]) J.out_fwd[1] += cofs;
+		if (J.out_snap) J.out_snap = (J.snap_flag[cand] != 0u) ? J.out_snap + cofs : nullptr;
+	}
 	const u32 R = c.R, n = c.n;
 	const int nb = (int)gridDim.x, b = (int)blockIdx.x;
 	const u32 c0 = (u32)b * CC;
@@ -481,7 +496,15 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	const int E = (!J.transformed || single) ? 0 : ((b == 0 && J.lower != LOWER_NONE) ? 8 : 4);
 	const int WU = CC + E, ng = WU / 4;
 	const int tid = (int)threadIdx.x, NT = (int)blockDim.x;
-	const int lb = c.lbase;
+	if (tid == 0)
+	{
+		if (J.cand != nullptr) cc = J.cand[cand];
+		else
+		{
+			cc.lbase = c.lbase;
+			for (int k = 0; k < AB_MAXK; ++k) { cc.rbase[k] = c.rbase[k]; cc.rbase_pck[k] = c.rbase_pck[k]; }
+		}
+	}
 
 	auto gcol = [&](int u) -> u32 { return (u < E) ? ((b == 0) ? R - (u32)E + (u32)u : c0 - (u32)E + (u32)u) : c0 + (u32)(u - E); };
 
@@ -501,6 +524,7 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	}
 	if (tid == 0) decision = 0;
 	__syncthreads();
+	const int lb = cc.lbase;
 
 	if (J.transformed)
 	{
@@ -538,7 +562,7 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 #pragma unroll
 				for (int k = 0; k < K; ++k) rr[k] = mont_mul(xv[k][j], c.norm[k], c.p[k], c.q[k]);
 				const Big<K> V = garner<K>(c, rr);
-				f = big_add<K>(f, (J.a == 1u) ? V : big_mul_u32<K>(V, J.a));
+				f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
 				if (J.sub != nullptr)
 				{
 #pragma unroll
@@ -593,7 +617,7 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 				dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
 			}
 			u32 res[4][K];
-			const i32 top = carry_phase2<K, PCK>(c, f, dg, res);
+			const i32 top = carry_phase2<K, PCK>(c, lb, cc.rbase, f, dg, res);
 			const bool is_last = (row == H - 1) && (u4 == ng - 1) && (b == nb - 1);
 			if ((is_last || !store) && top >= (i32)(1u << lb)) decision = 1;
 			if (store)
@@ -615,7 +639,7 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 				if (b == nb - 1)
 				{
 					u32 & t = tile[(k * H + H - 1) * TW + WU - 1];
-					t = sub_mod(t, c.rbase_pck[k], p);
+					t = sub_mod(t, cc.rbase_pck[k], p);
 				}
 				if (b == 0)
 				{
@@ -635,13 +659,15 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	// ---- outputs: normal form, then the first LA forward levels of the next
 	// product, computed in place (the second domain reloads the normal form
 	// from global memory)
-	if (J.out_norm != nullptr)
+	if (J.out_norm != nullptr || J.out_snap != nullptr)
 	{
 		for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
 		{
 			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
 			const uint4 val = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + E + 4 * u4);
-			*reinterpret_cast<uint4 *>(J.out_norm + (size_t)k * n + (size_t)row * R + c0 + 4 * u4) = val;
+			const size_t o = (size_t)k * n + (size_t)row * R + c0 + 4 * u4;
+			if (J.out_norm) *reinterpret_cast<uint4 *>(J.out_norm + o) = val;
+			if (J.out_snap) *reinterpret_cast<uint4 *>(J.out_snap + o) = val;
 		}
 		__syncthreads();
 	}
@@ -693,7 +719,7 @@ size_t colpass_smem(const Geometry & g, int K)
 }
 
 template <int LOG_R>
-static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s)
+static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	const u32 R = 1u << LOG_R;
 	const size_t smem = sizeof(u32) * (R + R / 16);
@@ -704,31 +730,32 @@ static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs
 		if (e != cudaSuccess) return e;
 		attr = true;
 	}
-	const dim3 grid((unsigned)(c.K * g.H), (unsigned)njobs);
+	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
+	const dim3 grid((unsigned)(c.K * g.H), (unsigned)njobs, (unsigned)ncand);
 	k_rowpass<LOG_R><<<grid, RowCfg<LOG_R>::NT, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
 
-cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s)
+cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	switch (g.LB + 1)
 	{
-	case 5: return rowpass_t<5>(g, c, jobs, njobs, s);
-	case 6: return rowpass_t<6>(g, c, jobs, njobs, s);
-	case 7: return rowpass_t<7>(g, c, jobs, njobs, s);
-	case 8: return rowpass_t<8>(g, c, jobs, njobs, s);
-	case 9: return rowpass_t<9>(g, c, jobs, njobs, s);
-	case 10: return rowpass_t<10>(g, c, jobs, njobs, s);
-	case 11: return rowpass_t<11>(g, c, jobs, njobs, s);
-	case 12: return rowpass_t<12>(g, c, jobs, njobs, s);
-	case 13: return rowpass_t<13>(g, c, jobs, njobs, s);
-	case 14: return rowpass_t<14>(g, c, jobs, njobs, s);
+	case 5: return rowpass_t<5>(g, c, jobs, njobs, s, ncand);
+	case 6: return rowpass_t<6>(g, c, jobs, njobs, s, ncand);
+	case 7: return rowpass_t<7>(g, c, jobs, njobs, s, ncand);
+	case 8: return rowpass_t<8>(g, c, jobs, njobs, s, ncand);
+	case 9: return rowpass_t<9>(g, c, jobs, njobs, s, ncand);
+	case 10: return rowpass_t<10>(g, c, jobs, njobs, s, ncand);
+	case 11: return rowpass_t<11>(g, c, jobs, njobs, s, ncand);
+	case 12: return rowpass_t<12>(g, c, jobs, njobs, s, ncand);
+	case 13: return rowpass_t<13>(g, c, jobs, njobs, s, ncand);
+	case 14: return rowpass_t<14>(g, c, jobs, njobs, s, ncand);
 	default: return cudaErrorInvalidValue;
 	}
 }
 
 template <int LOG_H, int K, int PCK>
-static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s)
+static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	const size_t smem = colpass_smem(g, K);
 	static bool attr = false;
@@ -738,34 +765,35 @@ static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs
 		if (e != cudaSuccess) return e;
 		attr = true;
 	}
-	const dim3 grid(g.R / CC, (unsigned)njobs);
+	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
+	const dim3 grid(g.R / CC, (unsigned)njobs, (unsigned)ncand);
 	k_colpass<LOG_H, K, PCK><<<grid, COL_THREADS, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
 
 template <int K, int PCK>
-static cudaError_t colpass_k(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s)
+static cudaError_t colpass_k(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	switch (g.LA)
 	{
-	case 1: return colpass_t<1, K, PCK>(g, c, jobs, njobs, s);
-	case 2: return colpass_t<2, K, PCK>(g, c, jobs, njobs, s);
-	case 3: return colpass_t<3, K, PCK>(g, c, jobs, njobs, s);
-	case 4: return colpass_t<4, K, PCK>(g, c, jobs, njobs, s);
-	case 5: return colpass_t<5, K, PCK>(g, c, jobs, njobs, s);
-	case 6: return colpass_t<6, K, PCK>(g, c, jobs, njobs, s);
+	case 1: return colpass_t<1, K, PCK>(g, c, jobs, njobs, s, ncand);
+	case 2: return colpass_t<2, K, PCK>(g, c, jobs, njobs, s, ncand);
+	case 3: return colpass_t<3, K, PCK>(g, c, jobs, njobs, s, ncand);
+	case 4: return colpass_t<4, K, PCK>(g, c, jobs, njobs, s, ncand);
+	case 5: return colpass_t<5, K, PCK>(g, c, jobs, njobs, s, ncand);
+	case 6: return colpass_t<6, K, PCK>(g, c, jobs, njobs, s, ncand);
 	default: return cudaErrorInvalidValue;
 	}
 }
 
-cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s)
+cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	switch (c.K)
 	{
-	case 2: return colpass_k<2, 1>(g, c, jobs, njobs, s);
-	case 3: return colpass_k<3, 2>(g, c, jobs, njobs, s);
-	case 4: return colpass_k<4, 2>(g, c, jobs, njobs, s);
-	case 5: return colpass_k<5, 4>(g, c, jobs, njobs, s);
+	case 2: return colpass_k<2, 1>(g, c, jobs, njobs, s, ncand);
+	case 3: return colpass_k<3, 2>(g, c, jobs, njobs, s, ncand);
+	case 4: return colpass_k<4, 2>(g, c, jobs, njobs, s, ncand);
+	case 5: return colpass_k<5, 4>(g, c, jobs, njobs, s, ncand);
 	default: return cudaErrorInvalidValue;
 	}
 }

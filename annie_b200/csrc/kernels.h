@@ -19,12 +19,17 @@ namespace ab
 
 enum RowMode { ROW_FWD_ONLY = 0, ROW_SQUARE = 1, ROW_MUL = 2 };
 
+// Batches: blockIdx.z selects a candidate; its buffers are at +z*stride
+// words (twiddles are shared).  `active` (nullable) holds one word per
+// candidate, 0 = skip it.
 struct RowJob
 {
 	u32 * x;          // K x n buffer, rows transformed in place
 	const u32 * xp;   // ROW_MUL: pre-transformed operand (same layout)
 	const u32 * w;    // twiddles of the domain: per prime n words, w (n/2) || wi (n/2)
 	int mode;
+	size_t stride;
+	const u32 * active;
 };
 struct RowJobs { RowJob j[2]; };
 
@@ -42,6 +47,11 @@ struct ColJob
 	u32 * out_norm;      // normal-form result (nullable)
 	u32 * out_fwd[2];    // first LA forward levels of the result, per domain (nullable)
 	const u32 * w_out[2];
+	size_t stride;       // words between candidates (batches)
+	const u32 * mult;    // per candidate: the carry multiplier a, 0 = inactive (nullable: use `a`)
+	const CandConst * cand;  // per-candidate digit constants (nullable: those of TConst)
+	u32 * out_snap;      // per candidate: also store the normal form here when snap_flag[z] != 0
+	const u32 * snap_flag;
 };
 struct ColJobs { ColJob j[2]; };
 
@@ -58,7 +68,7 @@ bool make_geometry(int ln, int lb_override, Geometry & g);
 // Column-pass scratch in shared memory, bytes.
 size_t colpass_smem(const Geometry & g, int K);
 
-cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s);
-cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s);
+cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
+cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
 
 } // namespace ab

@@ -1,0 +1,341 @@
+// PRP test driver (include/annie_b200_driver.h).
+//
+// Follows the reference driver annie::check (src/annie.h:217-430): trivial
+// cases, base selection, left-to-right exponentiation with the multiplier
+// fused into square_mul, the Gerbicz-Li product d(t) every B iterations, the
+// final Gerbicz-Li identity a^res d(t)^(2^B) = d(t+1), RES64, checkpoint
+// files.  Added (the reference only checks at the end and cannot recover):
+// a periodic Gerbicz-Li check every `gl_check_blocks` blocks that rolls back
+// to the last verified (Reg0, Reg1) on mismatch, and host-side fault
+// injection (one register word changed between two launches).
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <sys/stat.h>
+
+#include "gmp.h"
+#include "transformCUDA.h"
+#include "../../include/annie_b200_driver.h"
+
+namespace
+{
+std::atomic<bool> g_quit{false};
+
+int ilog2_32(uint32_t n) { return (n == 0) ? -1 : (31 - __builtin_clz(n)); }
+
+// Gerbicz-Li block size for an exponent of `size` bits (src/annie.h:97-101)
+int gl_block_size(size_t size)
+{
+	const size_t L = size_t(2) << (ilog2_32(uint32_t(size)) / 2);
+	return int((size - 1) / L) + 1;
+}
+
+std::string hex64(uint64_t u)
+{
+	char b[32];
+	std::snprintf(b, sizeof(b), "%016llX", (unsigned long long)u);
+	return b;
+}
+
+// sum of the B-bit chunks of e (src/annie.h:368-375)
+void chunk_sum(mpz_t res, const mpz_t e_in, int B)
+{
+	mpz_t e, t; mpz_init_set(e, e_in); mpz_init(t);
+	mpz_set_ui(res, 0);
+	while (mpz_sgn(e) != 0)
+	{
+		mpz_fdiv_r_2exp(t, e, (mp_bitcnt_t)B);
+		mpz_add(res, res, t);
+		mpz_fdiv_q_2exp(e, e, (mp_bitcnt_t)B);
+	}
+	mpz_clears(e, t, nullptr);
+}
+
+// r0 = a^res * r_d^(2^B) on the transform (src/annie.h:377-395): fused
+// multipliers for the bits of res above B, times register d, then B more
+// squarings with the low bits of res.
+int64_t gl_power(transformCUDA & t, const mpz_t res, int32_t a, int B, size_t d)
+{
+	int64_t sq = 0;
+	const int rs = int(mpz_sizeinbase(res, 2));
+	t.set1();
+	for (int i = rs - 1; i >= B; --i) { t.square_mul(mpz_tstbit(res, (mp_bitcnt_t)i) ? a : 1); ++sq; }
+	t.mul(transform::Reg0, d);
+	for (int i = B - 1; i >= 0; --i) { t.square_mul(((i < rs) && mpz_tstbit(res, (mp_bitcnt_t)i)) ? a : 1); ++sq; }
+	return sq;
+}
+
+struct Checkpointer
+{
+	std::string path;
+
+	// format of src/annie.h:162-181: int version = 1, int i, double elapsed,
+	// transform payload, CRC seal
+	bool save(transformCUDA & t, int i, double elapsed) const
+	{
+		const std::string cur = path, old = path + ".old", nw = path + ".new";
+		{
+			ckfile f(nw, "wb");
+			if (!f.exists()) return false;
+			const int version = 1;
+			f.write(&version, sizeof(version));
+			f.write(&i, sizeof(i));
+			f.write(&elapsed, sizeof(elapsed));
+			t.save_checkpoint(f);
+			f.write_seal();
+		}
+		std::remove(old.c_str());
+		struct stat s;
+		if (stat(cur.c_str(), &s) == 0) std::rename(cur.c_str(), old.c_str());
+		return std::rename(nw.c_str(), cur.c_str()) == 0;
+	}
+
+	bool read_one(transformCUDA & t, const std::string & name, int & i, double & elapsed) const
+	{
+		ckfile f(name, "rb");
+		if (!f.exists()) return false;
+		int version = 0;
+		if (!f.read(&version, sizeof(version)) || version != 1) return false;
+		if (!f.read(&i, sizeof(i)) || !f.read(&elapsed, sizeof(elapsed))) return false;
+		if (!t.read_checkpoint(f)) return false;
+		return f.check_seal();
+	}
+
+	bool read(transformCUDA & t, int & i, double & elapsed) const
+	{
+		return read_one(t, path, i, elapsed) || read_one(t, path + ".old", i, elapsed);
+	}
+
+	void clear() const
+	{
+		std::remove(path.c_str());
+		std::remove((path + ".old").c_str());
+	}
+};
+
+int run(const mpz_t n, const ab_prp_options & o, ab_prp_result & r)
+{
+	using clk = std::chrono::steady_clock;
+	const auto t0 = clk::now();
+	auto elapsed = [&] { return std::chrono::duration<double>(clk::now() - t0).count(); };
+	const char * kind = o.euler ? "Euler" : "Fermat";
+
+	// ---- decided without the transform (src/annie.h:222-247)
+	if (mpz_sizeinbase(n, 2) <= 50 && mpz_cmp_ui(n, 999999999999999ul) <= 0)
+	{
+		const int pp = mpz_probab_prime_p(n, 20);
+		r.decided_early = 1;
+		r.is_prp = pp != 0;
+		std::snprintf(r.message, sizeof(r.message), "N is %s.", (pp == 2) ? "prime" : (pp == 1) ? "a probable prime" : "composite");
+		return 0;
+	}
+	if (mpz_even_p(n))
+	{
+		r.decided_early = 1;
+		std::snprintf(r.message, sizeof(r.message), "N is even.");
+		return 0;
+	}
+
+	// ---- base (src/annie.h:249-254)
+	int32_t a = 2;
+	if (o.euler)
+	{
+		while (mpz_si_kronecker(a, n) != -1)
+		{
+			++a;
+			const int32_t s = (int32_t)std::lround(std::sqrt(double(a)));
+			if (s * s == a) ++a;
+		}
+	}
+	else if (o.base != 0) a = o.base;
+	r.base = a;
+
+	transformCUDA t(n, a, o.device);
+	if (t.init_failed())
+	{
+		mpz_t f; mpz_init(f);
+		t.get_factor(f);
+		r.decided_early = 1;
+		char * s = mpz_get_str(nullptr, 10, f);
+		std::snprintf(r.message, sizeof(r.message), "%.200s divides N.", s);
+		free(s);
+		mpz_clear(f);
+		return 0;
+	}
+	const ab_params & p = t.params();
+	r.K = p.K; r.pck = p.pck; r.ln = p.ln; r.lbase = p.lbase;
+
+	mpz_t E; mpz_init(E);
+	mpz_sub_ui(E, n, 1);
+	if (o.euler) mpz_fdiv_q_2exp(E, E, 1);
+	const size_t ebits = mpz_sizeinbase(E, 2);
+	const int B = gl_block_size(ebits);
+	r.gl_block = B;
+
+	Checkpointer ck;
+	const bool use_ck = (o.checkpoint_path != nullptr && o.checkpoint_path[0] != 0);
+	if (use_ck) ck.path = o.checkpoint_path;
+
+	const int i0 = int(ebits) - 1;
+	int i_start = i0;
+	double restored = 0;
+	if (use_ck && ck.read(t, i_start, restored)) r.resumed = 1;
+	else
+	{
+		i_start = i0;
+		t.set1();
+		t.copy(transform::Reg1, transform::Reg0);        // d(t)
+	}
+
+	// last state known good: (Reg0, Reg1) and the loop index it was taken at
+	std::vector<uint8_t> vsnap = t.payload();
+	int vi = i_start + 1;
+	bool injected = false;
+	int blocks = 0, fails_in_row = 0;
+	double last_ck = elapsed();
+	mpz_t c, e, v1, v2; mpz_inits(c, e, v1, v2, nullptr);
+
+	for (int i = i_start; i >= 0; --i)
+	{
+		if (g_quit.load(std::memory_order_relaxed))
+		{
+			if (use_ck) ck.save(t, i, restored + elapsed());
+			mpz_clears(E, c, e, v1, v2, nullptr);
+			r.seconds = elapsed();
+			std::snprintf(r.message, sizeof(r.message), "Test was aborted.");
+			return 2;
+		}
+		if (use_ck && o.checkpoint_seconds > 0 && elapsed() - last_ck >= o.checkpoint_seconds)
+		{
+			ck.save(t, i, restored + elapsed());
+			last_ck = elapsed();
+		}
+
+		t.square_mul(mpz_tstbit(E, (mp_bitcnt_t)i) ? a : 1);
+		++r.squarings;
+
+		if (!injected && (int64_t)i == o.inject_iteration)
+		{
+			// host-side fault: one residue of Reg0 moves by one, between two launches
+			const size_t words = (size_t)p.K << p.ln;
+			std::vector<uint32_t> reg(words);
+			if (ab_read_register(t.handle(), 0, reg.data(), words) != AB_OK) throw std::runtime_error(ab_last_error());
+			const size_t w = o.inject_word % words;
+			reg[w] = (reg[w] == 0) ? 1u : reg[w] - 1u;
+			if (ab_write_register(t.handle(), 0, reg.data(), words) != AB_OK) throw std::runtime_error(ab_last_error());
+			injected = true;
+		}
+
+		if ((i % B == 0) && (i / B != 0))
+		{
+			const bool check = (o.gl_check_blocks > 0) && (++blocks >= o.gl_check_blocks);
+			if (check) t.copy(transform::Reg2, transform::Reg1);      // d before this block's factor
+			t.mul(transform::Reg1, transform::Reg0);                  // d(t)
+			if (check)
+			{
+				// d_now = d_prev^(2^B) a^C, C = sum of the B-bit chunks of E >> i
+				blocks = 0;
+				++r.gl_checks;
+				mpz_fdiv_q_2exp(e, E, (mp_bitcnt_t)i);
+				chunk_sum(c, e, B);
+				const std::vector<uint8_t> stash = t.payload();
+				r.squarings += gl_power(t, c, a, B, transform::Reg2);
+				t.get(v1, transform::Reg0);
+				t.load_payload(stash);
+				t.get(v2, transform::Reg1);
+				if (mpz_cmp(v1, v2) == 0)
+				{
+					vsnap = stash;
+					vi = i;
+					fails_in_row = 0;
+				}
+				else
+				{
+					++r.gl_failures;
+					++r.rollbacks;
+					if (++fails_in_row > 8)
+					{
+						// the same stretch keeps failing: not a transient fault
+						mpz_clears(E, c, e, v1, v2, nullptr);
+						r.seconds = elapsed();
+						std::snprintf(r.message, sizeof(r.message), "Validation failed! (repeated Gerbicz-Li mismatch)");
+						return 1;
+					}
+					t.load_payload(vsnap);
+					i = vi;          // resumes at vi - 1
+					continue;
+				}
+			}
+		}
+	}
+
+	// ---- end of test (src/annie.h:343-403)
+	t.copy(transform::Reg2, transform::Reg0);
+	t.mul(transform::Reg2, transform::Reg1);                          // d(t+1)
+	t.get(v1, transform::Reg0);
+	if (o.euler)
+	{
+		mpz_add_ui(v1, v1, 1);
+		if (mpz_cmp(v1, n) >= 0) mpz_sub(v1, v1, n);
+		t.square_mul(1);
+		++r.squarings;
+	}
+	else mpz_sub_ui(v1, v1, 1);
+	r.is_prp = (mpz_sgn(v1) == 0);
+	t.get(v1, transform::Reg0);
+	r.res64 = (mpz_size(v1) != 0) ? (uint64_t)mpz_getlimbn(v1, 0) : 0;
+
+	chunk_sum(c, E, B);
+	r.squarings += gl_power(t, c, a, B, transform::Reg1);
+	t.get(v1, transform::Reg0);
+	t.get(v2, transform::Reg2);
+	const bool ok = (mpz_cmp(v1, v2) == 0);
+	mpz_clears(E, c, e, v1, v2, nullptr);
+	r.seconds = elapsed();
+	if (ok)
+	{
+		if (r.is_prp) std::snprintf(r.message, sizeof(r.message), "N is a %s probable prime, a = %d.", kind, a);
+		else std::snprintf(r.message, sizeof(r.message), "N is composite, res64 = %s, a = %d.", hex64(r.res64).c_str(), a);
+		if (use_ck) ck.clear();
+		return 0;
+	}
+	std::snprintf(r.message, sizeof(r.message), "Validation failed!");
+	return 1;
+}
+} // namespace
+
+extern "C" {
+
+void ab_prp_options_default(ab_prp_options * o)
+{
+	std::memset(o, 0, sizeof(*o));
+	o->inject_iteration = -1;
+	o->checkpoint_seconds = 600;
+}
+
+int ab_prp_check(const uint64_t * Nl, size_t nlimbs, const ab_prp_options * opt, ab_prp_result * out)
+{
+	if (Nl == nullptr || nlimbs == 0 || out == nullptr) return -1;
+	std::memset(out, 0, sizeof(*out));
+	ab_prp_options o;
+	if (opt) o = *opt; else ab_prp_options_default(&o);
+	mpz_t n; mpz_init(n);
+	mpz_import(n, nlimbs, -1, 8, 0, 0, Nl);
+	try { out->status = run(n, o, *out); }
+	catch (const std::exception & e)
+	{
+		out->status = -1;
+		std::snprintf(out->message, sizeof(out->message), "error: %.200s", e.what());
+	}
+	mpz_clear(n);
+	return out->status;
+}
+
+void ab_prp_quit(void) { g_quit.store(true, std::memory_order_relaxed); }
+void ab_prp_reset_quit(void) { g_quit.store(false, std::memory_order_relaxed); }
+
+}

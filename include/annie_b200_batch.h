@@ -1,0 +1,76 @@
+/*
+ * annie_b200 batches and the continuous-batching runner -- no counterpart in
+ * the reference, which tests one number at a time (src/annie.h:217-430).
+ *
+ * A batch is a size class (K, pck, ln) of `capacity` slots.  Each loaded slot
+ * is a regular ab_transform (returned by ab_batch_slot: use it with ab_set1,
+ * ab_copy, ab_mul, ab_get, ...; never ab_destroy it).  ab_batch_steps runs
+ * `steps` squarings of every slot together from a captured CUDA graph.
+ *
+ * The runner queues PRP tests, admits them into batches as slots and HBM
+ * budget free up, and runs each to its result (same verdict and RES64 as
+ * ab_prp_check on the number alone).
+ */
+#ifndef ANNIE_B200_BATCH_H
+#define ANNIE_B200_BATCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "annie_b200.h"
+#include "annie_b200_driver.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ab_batch ab_batch;
+
+/* Device bytes one slot of the class holds. */
+size_t ab_batch_slot_bytes(const ab_params * cls);
+int ab_batch_create(int device, const ab_params * cls, int capacity, int max_steps, ab_batch ** out);
+void ab_batch_destroy(ab_batch * b);
+/* Sets up slot `slot` for N and base a (the digit size may differ between
+   slots); N must fall in the class (K, pck, ln) by the factory rule. */
+int ab_batch_load(ab_batch * b, int slot, const uint64_t * N, size_t nlimbs, int32_t a, int * init_failed);
+ab_transform * ab_batch_slot(ab_batch * b, int slot);
+int ab_batch_release(ab_batch * b, int slot);
+/* mult[s * capacity + slot]: multiplier of squaring s for the slot (a or 1;
+   0 = the slot sits this step out).  snap (nullable, same shape): after that
+   squaring, keep Reg0 for the Gerbicz-Li product; ab_batch_gl_mul(slot) then
+   does Reg1 *= kept value. */
+int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t * snap);
+int ab_batch_gl_mul(ab_batch * b, int slot);
+/* Row levels per row pass (0 = default split); used by the autotuner. */
+int ab_batch_set_geometry(ab_batch * b, int lb);
+int ab_batch_synchronize(ab_batch * b);
+int ab_batch_launch_count(const ab_batch * b, uint64_t * count);
+
+typedef struct ab_runner ab_runner;
+
+typedef struct
+{
+	int device;
+	size_t hbm_budget_bytes;   /* device memory the runner may give to batches */
+	int max_slots_per_class;
+	int chunk;                 /* squarings per graph launch */
+} ab_runner_options;
+
+void ab_runner_options_default(ab_runner_options * o);
+int ab_runner_create(const ab_runner_options * o, ab_runner ** out);
+void ab_runner_destroy(ab_runner * r);
+/* Queues a PRP test (Fermat base `base`, 0 = 2; or Euler). */
+int ab_runner_submit(ab_runner * r, const uint64_t * N, size_t nlimbs, int euler, int32_t base, uint64_t tag);
+/* Admits queued tests into free slots, then runs one chunk of every batch and
+   the host steps of the tests that reached the end of a phase. */
+int ab_runner_advance(ab_runner * r, int * active, int * queued);
+/* Pops one finished test; returns 1 if one was available, 0 otherwise. */
+int ab_runner_poll(ab_runner * r, uint64_t * tag, ab_prp_result * out);
+/* Squarings executed for tests since creation (all slots). */
+int ab_runner_stats(const ab_runner * r, uint64_t * squarings, uint64_t * launches, int * batches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

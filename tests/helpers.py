@@ -45,3 +45,31 @@ def random_residues(K, ln, seed):
     rng = np.random.default_rng(seed)
     n = 1 << ln
     return np.concatenate([rng.integers(0, PRIMES[k], size=n, dtype=np.uint64).astype(np.uint32) for k in range(K)])
+
+
+SMALL_PRIMES = [p for p in range(3, 2000) if all(p % q for q in range(2, int(p ** 0.5) + 1))]
+
+
+def coprime_to_small(N):
+    return all(N % p for p in SMALL_PRIMES)
+
+
+def random_N(bits, seed):
+    """First draw of the seeded generator with no prime factor below 2000
+    (the rule of tests/golden/make_golden.py)."""
+    rng = Xoshiro256ss(seed)
+    while True:
+        N = rng.random_odd(bits)
+        if coprime_to_small(N):
+            return N
+
+
+def proth_N(n, seed):
+    """k*2^n + 1 with k odd in [2^19, 2^20) from the seeded generator, no prime factor below 2000."""
+    from annie_b200.synth import proth
+    rng = Xoshiro256ss(seed)
+    while True:
+        k = rng.uniform(1 << 19, 1 << 20) | 1
+        N = proth(k, n)
+        if coprime_to_small(N):
+            return k, N

@@ -9,8 +9,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "annie_b200.h")).read()
-    return sorted(set(re.findall(r"\b(ab_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in sorted(os.listdir(inc)):
+        if f.endswith(".h"):
+            text = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, f)).read(), flags=re.S)
+            names |= set(re.findall(r"\b(ab_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_and_binding_agree():

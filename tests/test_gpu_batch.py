@@ -1,0 +1,127 @@
+"""GPU tests of batches (many candidates squared together from a captured
+CUDA graph) and of the continuous-batching runner: every candidate's result
+must be the same in the mix as alone, bit for bit."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import annie_b200 as A
+from annie_b200.synth import Xoshiro256ss
+from helpers import proth_N, random_N
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _same_class_numbers(cls, count, lo, hi, seed):
+    rng = Xoshiro256ss(seed)
+    out = []
+    while len(out) < count:
+        bits = rng.uniform(lo, hi)
+        N = rng.random_odd(bits)
+        p, failed = A.probe(N, 3)
+        if not failed and p[:3] == cls:
+            out.append((N, p))
+    return out
+
+
+def test_batch_slots_equal_single_transforms():
+    cls = (5, 4, 12)
+    nums = _same_class_numbers(cls, 5, 200000, 280000, 1)
+    assert len({p[3] for _, p in nums}) >= 1
+    b = A.Batch(cls + (0,), capacity=6, max_steps=16)
+    singles = []
+    for s, (N, p) in enumerate(nums):
+        assert not b.load(s, N, 3)
+        v = b.slot(s)
+        v.set1(); v.copy(1, 0)
+        t = A.Transform(N, 3)
+        t.set1(); t.copy(1, 0)
+        singles.append(t)
+    rng = np.random.default_rng(7)
+    for rnd in range(3):
+        steps = 16
+        mult = rng.choice([1, 3], size=(steps, 6)).astype(np.uint32)
+        mult[:, 5] = 0                      # slot 5 is empty
+        mult[steps - 3:, 2] = 0             # slot 2 sits the last steps out
+        snap = np.zeros((steps, 6), dtype=np.uint8)
+        snap[5, 1] = 1
+        b.steps(mult, snap)
+        b.gl_mul(1)
+        for s, t in enumerate(singles):
+            for i in range(steps):
+                if mult[i, s]:
+                    t.square_mul(int(mult[i, s]))
+                    if s == 1 and i == 5:
+                        t.copy(2, 0)
+            if s == 1:
+                t.mul(1, 2)
+        for s, t in enumerate(singles):
+            v = b.slot(s)
+            assert np.array_equal(v.read_register(0), t.read_register(0)), "slot %d Reg0, round %d" % (s, rnd)
+            assert np.array_equal(v.read_register(1), t.read_register(1)), "slot %d Reg1, round %d" % (s, rnd)
+    for s, t in enumerate(singles):
+        assert b.slot(s).get(0) == t.get(0)
+
+
+def _run_all(runner, limit=200000):
+    results = {}
+    for _ in range(limit):
+        active, queued = runner.advance()
+        for tag, r in runner.poll():
+            results[tag] = r
+        if active == 0 and queued == 0:
+            break
+    for tag, r in runner.poll():
+        results[tag] = r
+    return results
+
+
+def test_runner_matches_reference_golden_and_solo():
+    with open(os.path.join(HERE, "golden", "prp_vectors.json")) as f:
+        vec = [v for v in json.load(f) if not v.get("big")]
+    jobs = {}
+    for tag, v in enumerate(vec):
+        N = random_N(v["bits"], v["seed"]) if v["form"] == "random_odd" else proth_N(v["n"], v["seed"])[1]
+        jobs[tag] = (N, v)
+    r = A.Runner(chunk=32, max_slots_per_class=8)
+    for tag, (N, v) in jobs.items():
+        r.submit(N, euler=bool(v["euler"]), base=v["base"], tag=tag)
+    res = _run_all(r)
+    assert set(res) == set(jobs)
+    for tag, (N, v) in jobs.items():
+        got = res[tag]
+        assert got["status"] == 0, got["message"]
+        assert bool(got["is_prp"]) == v["is_prp"]
+        if v["res64"] is not None:
+            assert "%016X" % got["res64"] == v["res64"]
+        solo = A.prp_check(N, euler=bool(v["euler"]), base=v["base"])
+        assert (solo["res64"], solo["is_prp"]) == (got["res64"], got["is_prp"])
+
+
+def test_runner_continuous_admission_under_budget():
+    # room for 2 slots of the class at a time: the rest wait and are admitted as slots free up
+    nums = _same_class_numbers((5, 4, 10), 5, 50000, 70000, 3)
+    per = A.lib().ab_batch_slot_bytes(A.Params(5, 4, 10, 0))
+    r = A.Runner(chunk=64, max_slots_per_class=2, hbm_budget_bytes=2 * per)
+    for tag, (N, p) in enumerate(nums):
+        r.submit(N, base=3, tag=tag)
+    a, q = r.advance()
+    assert a == 2 and q == 3
+    res = _run_all(r)
+    assert len(res) == 5
+    for tag, (N, p) in enumerate(nums):
+        solo = A.prp_check(N, base=3)
+        assert res[tag]["res64"] == solo["res64"] and res[tag]["status"] == 0
+
+
+def test_runner_decides_trivial_cases():
+    r = A.Runner(chunk=16)
+    r.submit(1000003, tag=1)              # <= 15 digits: GMP decides (annie.h:222-237)
+    r.submit((1 << 4000) + 2, tag=2)      # even
+    res = _run_all(r, limit=10)
+    assert res[1]["decided_early"] == 1 and res[1]["is_prp"] == 1
+    assert res[2]["decided_early"] == 1 and "even" in res[2]["message"]
