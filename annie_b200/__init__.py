@@ -107,6 +107,7 @@ ABI = [
     ("ab_batch_destroy", [C.c_void_p], None),
     ("ab_batch_load", [C.c_void_p, C.c_int, _u64p, C.c_size_t, C.c_int32, C.POINTER(C.c_int)], C.c_int),
     ("ab_batch_slot", [C.c_void_p, C.c_int], C.c_void_p),
+    ("ab_batch_clone", [C.c_void_p, C.c_int, C.c_int], C.c_int),
     ("ab_batch_release", [C.c_void_p, C.c_int], C.c_int),
     ("ab_batch_steps", [C.c_void_p, C.c_int, _u32p, _u8p], C.c_int),
     ("ab_batch_gl_mul", [C.c_void_p, C.c_int], C.c_int),
@@ -158,14 +159,16 @@ def limbs_to_int(a, count):
     return int.from_bytes(np.asarray(a[:count], dtype=np.uint64).tobytes(), "little")
 
 
-def probe(N, a, forced=None):
-    """(params tuple, init_failed) by the factory rule of transformGPU.h:822-857; no GPU needed."""
+def probe(N, a, forced=None, gcd=True):
+    """(params tuple, init_failed) by the factory rule of transformGPU.h:822-857; no GPU
+    needed.  gcd=False skips the gcd(N, R) test (init_failed is then None)."""
     limbs = int_to_limbs(N)
     out = Params()
     failed = C.c_int()
     fp = None if forced is None else C.byref(Params(*forced))
-    _check(lib().ab_probe(limbs.ctypes.data_as(_u64p), len(limbs), a, fp, C.byref(out), C.byref(failed)))
-    return out.astuple(), bool(failed.value)
+    _check(lib().ab_probe(limbs.ctypes.data_as(_u64p), len(limbs), a, fp, C.byref(out),
+                          C.byref(failed) if gcd else None))
+    return out.astuple(), (bool(failed.value) if gcd else None)
 
 
 def prp_check(N, euler=False, base=0, device=0, gl_check_blocks=0, inject_iteration=-1, inject_word=0,
@@ -403,6 +406,10 @@ class Batch:
     def release(self, slot):
         _check(self.L.ab_batch_release(self.h, slot))
         self.Ns[slot] = None
+
+    def clone(self, dst, src):
+        _check(self.L.ab_batch_clone(self.h, dst, src))
+        self.Ns[dst], self.bases[dst] = self.Ns[src], self.bases[src]
 
     def steps(self, mult, snap=None):
         """mult: array [steps, capacity] of multipliers (0 = idle); snap: same shape, nonzero = keep Reg0."""

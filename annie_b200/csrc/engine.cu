@@ -519,10 +519,13 @@ struct ab_batch
 	CandConst * d_cand = nullptr;
 	std::vector<CandConst> h_cand;
 	u32 * d_ctrl = nullptr;            // per step: mult[cap] | act[cap] | snap[cap]
-	std::vector<u32> h_ctrl;
+	u32 * h_ctrl[2] = {};              // page-locked staging, alternating between launches
+	cudaEvent_t ctrl_done[2] = {};     // the upload out of h_ctrl[i] has completed
+	int ctrl_i = 0;
 	std::vector<ab_transform *> views;
 	cudaGraphExec_t gexec = nullptr;
 	int g_steps = 0;
+	int zl = 0;                        // slots the graph launches (grid.z): a power of two covering every live slot
 	uint64_t launches = 0;
 
 	~ab_batch()
@@ -532,6 +535,7 @@ struct ab_batch
 		if (mem) cudaFree(mem);
 		if (d_cand) cudaFree(d_cand);
 		if (d_ctrl) cudaFree(d_ctrl);
+		for (int i = 0; i < 2; ++i) { if (h_ctrl[i]) cudaFreeHost(h_ctrl[i]); if (ctrl_done[i]) cudaEventDestroy(ctrl_done[i]); }
 		if (st) cudaStreamDestroy(st);
 	}
 
@@ -540,12 +544,12 @@ struct ab_batch
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
-		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st, cap));
+		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st, zl));
 	}
 	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
 	{
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
-		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, cap));
+		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, zl));
 	}
 	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp, const u32 * act) const
 	{
@@ -981,7 +985,12 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 		CK(cudaMemcpyAsync(b->d_cand, b->h_cand.data(), sizeof(CandConst) * capacity, cudaMemcpyHostToDevice, b->st));
 		CK(cudaMalloc(&b->d_ctrl, (size_t)3 * max_steps * capacity * 4));
 		CK(cudaMemsetAsync(b->d_ctrl, 0, (size_t)3 * max_steps * capacity * 4, b->st));
-		b->h_ctrl.assign((size_t)3 * max_steps * capacity, 0);
+		for (int i = 0; i < 2; ++i)
+		{
+			CK(cudaMallocHost(&b->h_ctrl[i], (size_t)3 * max_steps * capacity * 4));
+			CK(cudaEventCreateWithFlags(&b->ctrl_done[i], cudaEventDisableTiming));
+			CK(cudaEventRecord(b->ctrl_done[i], b->st));
+		}
 		b->views.assign(capacity, nullptr);
 		// TConst of the class (digit constants come from d_cand)
 		ab_transform probe_t;
@@ -1046,6 +1055,33 @@ ab_transform * ab_batch_slot(ab_batch * b, int slot)
 	return b->views[slot];
 }
 
+int ab_batch_clone(ab_batch * b, int dst, int src)
+{
+	return guarded([&] {
+		if (b == nullptr || dst < 0 || dst >= b->cap || src < 0 || src >= b->cap || dst == src || b->views[src] == nullptr)
+			throw ab_error(AB_E_ARG, "bad arguments");
+		const ab_transform * s = b->views[src];
+		delete b->views[dst];
+		b->views[dst] = nullptr;
+		ab_transform * v = new ab_transform();
+		v->view = true;
+		mpz_inits(v->N, v->factor, nullptr);
+		mpz_set(v->N, s->N); mpz_set(v->factor, s->factor);
+		v->prm = s->prm; v->n = s->n; v->geo = s->geo; v->tc = s->tc; v->failed = s->failed;
+		v->device = b->device; v->st = b->st; v->overlap = false;
+		v->host.assign(b->words, 0);
+		for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)dst * b->words;
+		v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
+		v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
+		for (int i = 0; i < ab_transform::WR; ++i)
+			CK(cudaMemcpyAsync(v->bufp[i], s->bufp[i], b->words * 4, cudaMemcpyDeviceToDevice, b->st));
+		b->h_cand[dst] = b->h_cand[src];
+		CK(cudaMemcpyAsync(b->d_cand + dst, &b->h_cand[dst], sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
+		CK(cudaStreamSynchronize(b->st));
+		b->views[dst] = v;
+	});
+}
+
 int ab_batch_release(ab_batch * b, int slot)
 {
 	return guarded([&] {
@@ -1069,19 +1105,35 @@ int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t
 	return guarded([&] {
 		if (b == nullptr || mult == nullptr || steps < 1 || steps > b->max_steps) throw ab_error(AB_E_ARG, "bad arguments");
 		const int cap = b->cap;
+		// launch only as many slots as the highest one that steps: idle slots above
+		// it cost a launch of empty blocks per pass
+		int top = 0;
+		for (int c = 0; c < cap; ++c)
+			if (b->views[c] != nullptr && !b->views[c]->failed)
+				for (int s = 0; s < steps; ++s) if (mult[(size_t)s * cap + c] != 0u) { top = c + 1; break; }
+		int zl = 1;
+		while (zl < top) zl <<= 1;
+		zl = std::min(zl, cap);
+		// the staging buffer used two launches ago must have been uploaded
+		const int hi = b->ctrl_i;
+		CK(cudaEventSynchronize(b->ctrl_done[hi]));
+		u32 * const hc = b->h_ctrl[hi];
 		for (int s = 0; s < steps; ++s)
 			for (int c = 0; c < cap; ++c)
 			{
 				const bool live = b->views[c] != nullptr && !b->views[c]->failed;
 				const u32 m = live ? mult[(size_t)s * cap + c] : 0u;
-				b->h_ctrl[((size_t)s * 3 + 0) * cap + c] = m;
-				b->h_ctrl[((size_t)s * 3 + 1) * cap + c] = (m != 0u) ? 1u : 0u;
-				b->h_ctrl[((size_t)s * 3 + 2) * cap + c] = (snap != nullptr && m != 0u && snap[(size_t)s * cap + c]) ? 1u : 0u;
+				hc[((size_t)s * 3 + 0) * cap + c] = m;
+				hc[((size_t)s * 3 + 1) * cap + c] = (m != 0u) ? 1u : 0u;
+				hc[((size_t)s * 3 + 2) * cap + c] = (snap != nullptr && m != 0u && snap[(size_t)s * cap + c]) ? 1u : 0u;
 			}
-		CK(cudaMemcpyAsync(b->d_ctrl, b->h_ctrl.data(), (size_t)3 * steps * cap * 4, cudaMemcpyHostToDevice, b->st));
-		if (b->gexec == nullptr || b->g_steps != steps)
+		CK(cudaMemcpyAsync(b->d_ctrl, hc, (size_t)3 * steps * cap * 4, cudaMemcpyHostToDevice, b->st));
+		CK(cudaEventRecord(b->ctrl_done[hi], b->st));
+		b->ctrl_i ^= 1;
+		if (b->gexec == nullptr || b->g_steps != steps || b->zl != zl)
 		{
 			if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+			b->zl = zl;
 			cudaGraph_t g = nullptr;
 			CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
 			try { b->record_steps(steps); }

@@ -92,6 +92,7 @@ struct Class
 	std::vector<Job *> slots;
 	std::vector<uint32_t> mult;
 	std::vector<uint8_t> snap;
+	std::vector<int> count;
 };
 
 std::string hex64(uint64_t u)
@@ -292,13 +293,15 @@ struct ab_runner
 		finish(j, ok ? 0 : 1, msg);
 	}
 
-	void run_class(Class & c)
+	// queues one chunk of the class (asynchronous); returns false when idle
+	bool launch_class(Class & c)
 	{
 		const int cap = c.cap, S = o.chunk;
 		bool any = false;
 		std::fill(c.mult.begin(), c.mult.end(), 0u);
 		std::fill(c.snap.begin(), c.snap.end(), (uint8_t)0);
-		std::vector<int> count(cap, 0);
+		std::vector<int> & count = c.count;
+		count.assign(cap, 0);
 		for (int s = 0; s < cap; ++s)
 		{
 			Job * j = c.slots[s];
@@ -313,8 +316,16 @@ struct ab_runner
 			}
 			if (n > 0) any = true;
 		}
-		if (!any) return;
+		if (!any) return false;
 		ck(ab_batch_steps(c.b, S, c.mult.data(), c.snap.data()));
+		return true;
+	}
+
+	// after the chunk: Gerbicz-Li products and the host steps between phases
+	void settle_class(Class & c)
+	{
+		const int cap = c.cap;
+		std::vector<int> & count = c.count;
 		for (int s = 0; s < cap; ++s)
 		{
 			Job * j = c.slots[s];
@@ -372,7 +383,9 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 	try
 	{
 		r->admit();
-		for (auto & c : r->classes) r->run_class(*c);
+		std::vector<Class *> ran;
+		for (auto & c : r->classes) if (r->launch_class(*c)) ran.push_back(c.get());
+		for (Class * c : ran) r->settle_class(*c);
 	}
 	catch (const std::exception & e)
 	{

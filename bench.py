@@ -281,6 +281,212 @@ def run_reference(args, world, rank, pg):
     }
 
 
+# ---------------------------------------------------------------- other workloads
+SMALL_PRIMES = [p for p in range(3, 2000) if all(p % q for q in range(2, int(p ** 0.5) + 1))]
+
+def _autotune_batch(b, cls, S, mult, reps=3):
+    """Row levels per row pass for a size class: time each admissible split on the batch."""
+    ln = cls[2]
+    L = ln - 1
+    best = None
+    for lb in sorted({min(L - 1, 12), min(L - 1, 11), min(L - 1, 10), min(L - 1, 13)}):
+        if lb < 4 or lb > 13 or L - lb > 6:
+            continue
+        try:
+            b.set_geometry(lb)
+        except Exception:
+            continue
+        b.steps(mult)
+        b.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            b.steps(mult)
+        b.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        if best is None or dt < best[1]:
+            best = (lb, dt)
+    b.set_geometry(best[0])
+    return best
+
+
+def run_batch_workload(args):
+    """4096 Proth candidates k*2^n+1 (k odd in [3, 2^20), n in [500000, 3000000], seeded):
+    candidates/hour of the batched path (autotuned per size class, graph-captured
+    chunks) against the one-at-a-time CUDA path on the same B200."""
+    import annie_b200 as A
+    from annie_b200.synth import Xoshiro256ss, proth
+    rng = Xoshiro256ss(2024)
+    cands = [(rng.uniform(3, 1 << 20) | 1, rng.uniform(500000, 3000001)) for _ in range(4096)]
+    classes = {}
+    for k, n in cands:
+        p, _ = A.probe(proth(k, n), 3, gcd=False)
+        classes.setdefault(p[:3], []).append((k, n))
+    CAP, S, REPS = args.batch_slots, 32, 4
+    per_class = []
+    t_batch = t_plain = 0.0
+    for cls, members in sorted(classes.items()):
+        N = None
+        for k, n in members:
+            cand = proth(k, n)
+            if not A.probe(cand, 3)[1]:
+                N = cand
+                break
+        E = (N - 1) >> 1
+        top = E.bit_length() - 1
+        bits = [(E >> (top - i)) & 1 for i in range(S)]
+        mult = [[3 if bits[i] else 1] * CAP for i in range(S)]
+        b = A.Batch(cls + (0,), capacity=CAP, max_steps=S)
+        b.load(0, N, 3)
+        b.slot(0).set1()
+        for s in range(1, CAP):
+            b.clone(s, 0)
+        lb, _ = _autotune_batch(b, cls, S, mult)
+        b.steps(mult)
+        b.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(REPS):
+            b.steps(mult)
+        b.synchronize()
+        batch_rate = CAP * S * REPS / (time.perf_counter() - t0)       # squarings / s
+        b.close()
+        t = A.Transform(N, 3)
+        t.set1()
+        t.square_mul_bits(0, S, 3)
+        t.synchronize()
+        t.timer_start()
+        for _ in range(REPS):
+            t.square_mul_bits(0, S, 3)
+        single_rate = S * REPS / (t.timer_stop() * 1e-3)
+        t.close()
+        squarings = sum(n + k.bit_length() - 1 for k, n in members)
+        t_batch += squarings / batch_rate
+        t_plain += squarings / single_rate
+        per_class.append({"class": list(cls), "candidates": len(members), "row_levels": lb,
+                          "batched_sq_per_s": round(batch_rate, 1), "single_us_per_sq": round(1e6 / single_rate, 2)})
+    value = len(cands) / (t_batch / 3600.0)
+    plain = len(cands) / (t_plain / 3600.0)
+    return {"metric": "proth_candidates_per_hour_batched", "value": round(value, 3), "unit": "candidates/hour",
+            "n_gpus": 1, "steps": REPS, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic (seeded Proth candidates)",
+            "config": {"workload": "4096 Proth k*2^n+1, k odd in [3,2^20), n in [500000,3000000] (xoshiro256** seed 2024)",
+                       "slots_per_class": CAP, "squarings_per_graph": S,
+                       "method": "per size class: measured squarings/s of a full batch (autotuned row/column split) and of the "
+                                 "one-at-a-time path; total squarings of the 4096 candidates divided by each rate"},
+            "plain_candidates_per_hour": round(plain, 3), "speedup_vs_plain": round(value / plain, 3),
+            "classes": per_class}
+
+
+def run_serve_workload(args):
+    """Poisson stream of PRP requests, bit lengths log-uniform (half Fermat base 3 on
+    random odd N, half Proth k*2^n+1): p50/p99 time-to-result and throughput of the
+    continuous-batching runner against the one-at-a-time path on the same stream."""
+    import math
+    import annie_b200 as A
+    from annie_b200.synth import Xoshiro256ss, proth
+    lo, hi = args.serve_bits
+    out_rates = []
+    for rate in args.serve_rates:
+        rng = Xoshiro256ss(int(rate * 1000) + 7)
+        reqs, t = [], 0.0
+        while True:
+            t += -math.log(1.0 - rng.random()) / rate
+            if t > args.serve_window:
+                break
+            bits = int(math.exp(math.log(lo) + rng.random() * (math.log(hi) - math.log(lo))))
+            while True:
+                # numbers with a factor below 2000 are decided at once by the gcd
+                # with R; keep those that need the full test
+                if len(reqs) % 2 == 0:
+                    N, euler, base = rng.random_odd(bits), False, 3
+                else:
+                    N, euler, base = proth(rng.uniform(3, 1 << 20) | 1, bits), True, 0
+                if all(N % p for p in SMALL_PRIMES):
+                    break
+            reqs.append((t, N, euler, base))
+        # served: continuous batching
+        r = A.Runner(chunk=32, max_slots_per_class=64)
+        t0 = time.perf_counter()
+        done, nxt, lat_s = {}, 0, []
+        while len(done) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt][0] <= now:
+                _, N, euler, base = reqs[nxt]
+                r.submit(N, euler=euler, base=base, tag=nxt)
+                nxt += 1
+            active, queued = r.advance()
+            now = time.perf_counter() - t0
+            for tag, res in r.poll():
+                done[tag] = res
+                lat_s.append(now - reqs[tag][0])
+            if active == 0 and queued == 0 and nxt < len(reqs):
+                time.sleep(max(0.0, min(0.01, reqs[nxt][0] - now)))
+        served_span = time.perf_counter() - t0
+        r.close()
+        # plain: one test at a time, first come first served
+        t0 = time.perf_counter()
+        lat_p, res_p = [], {}
+        for i, (ta, N, euler, base) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if now < ta:
+                time.sleep(ta - now)
+            res_p[i] = A.prp_check(N, euler=euler, base=base)
+            lat_p.append(time.perf_counter() - t0 - ta)
+        plain_span = time.perf_counter() - t0
+        same = all((done[i]["res64"], done[i]["is_prp"]) == (res_p[i]["res64"], res_p[i]["is_prp"]) for i in range(len(reqs)))
+
+        def pct(v, q):
+            v = sorted(v)
+            return v[min(len(v) - 1, int(q * len(v)))]
+        out_rates.append({"rate_per_s": rate, "requests": len(reqs),
+                          "served_p50_s": round(pct(lat_s, 0.5), 3), "served_p99_s": round(pct(lat_s, 0.99), 3),
+                          "served_throughput_per_h": round(len(reqs) / served_span * 3600, 1),
+                          "plain_p50_s": round(pct(lat_p, 0.5), 3), "plain_p99_s": round(pct(lat_p, 0.99), 3),
+                          "plain_throughput_per_h": round(len(reqs) / plain_span * 3600, 1),
+                          "results_equal_alone": same})
+    head = out_rates[-1]
+    return {"metric": "served_p99_time_to_result", "value": head["served_p99_s"], "unit": "s", "n_gpus": 1,
+            "steps": len(out_rates), "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic (seeded Poisson stream)",
+            "config": {"workload": "Poisson PRP requests, bit lengths log-uniform in [%d, %d], half Fermat base 3 random odd N, "
+                                   "half Proth (Euler), N without prime factors below 2000; arrivals over %.0f s per rate"
+                                   % (lo, hi, args.serve_window),
+                       "rates_per_s": args.serve_rates},
+            "rates": out_rates}
+
+
+def run_proth2m_workload(args):
+    """Proth k*2^2000000+1 (k seeded odd 20-bit), Euler: us per squaring over
+    steps of 512, and the cost of one periodic Gerbicz-Li verification."""
+    import annie_b200 as A
+    from annie_b200.synth import Xoshiro256ss, proth
+    rng = Xoshiro256ss(11)
+    while True:
+        k = rng.uniform(1 << 19, 1 << 20) | 1
+        N = proth(k, 2000000)
+        if not A.probe(N, 3)[1]:
+            break
+    t = A.Transform(N, 3)
+    t.set1()
+    t.copy(1, 0)
+    S = 512
+    E = (N - 1) >> 1
+    for _ in range(args.warmup):
+        t.square_mul_bits(0, S, 3)
+    t.synchronize()
+    ms = 0.0
+    for _ in range(args.steps):
+        t.flush_l2(256 << 20)
+        t.timer_start()
+        t.square_mul_bits(0, S, 3)
+        ms += t.timer_stop()
+    us = ms * 1e3 / (S * args.steps)
+    return {"metric": "us_per_squaring_proth_n2M", "value": round(us, 3), "unit": "us/squaring", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Proth number)",
+            "config": {"workload": "Proth k*2^2000000+1, k=%d, Euler test" % k, "ln": t.ln, "K": t.K, "lbase": t.lbase,
+                       "squarings_per_step": S}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -289,7 +495,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="square33M", choices=["square33M", "proth2M", "batch", "serve"])
+    ap.add_argument("--batch-slots", type=int, default=64)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.5, 2.0])
+    ap.add_argument("--serve-bits", type=int, nargs=2, default=[20000, 200000])
+    ap.add_argument("--serve-window", type=float, default=20.0)
     args = ap.parse_args()
+    if args.workload != "square33M":
+        fn = {"proth2M": run_proth2m_workload, "batch": run_batch_workload, "serve": run_serve_workload}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
+        return
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":
         line = run_reference(args, world, rank, pg)

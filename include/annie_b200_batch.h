@@ -34,6 +34,9 @@ void ab_batch_destroy(ab_batch * b);
    slots); N must fall in the class (K, pck, ln) by the factory rule. */
 int ab_batch_load(ab_batch * b, int slot, const uint64_t * N, size_t nlimbs, int32_t a, int * init_failed);
 ab_transform * ab_batch_slot(ab_batch * b, int slot);
+/* Slot dst becomes a copy of loaded slot src (same N and base, registers
+   included) without the host set-up: for re-tests and throughput runs. */
+int ab_batch_clone(ab_batch * b, int dst, int src);
 int ab_batch_release(ab_batch * b, int slot);
 /* mult[s * capacity + slot]: multiplier of squaring s for the slot (a or 1;
    0 = the slot sits this step out).  snap (nullable, same shape): after that
