@@ -61,7 +61,8 @@ class PrpResult(C.Structure):
 
 
 class RunnerOptions(C.Structure):
-    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots_per_class", C.c_int), ("chunk", C.c_int)]
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots_per_class", C.c_int), ("chunk", C.c_int),
+                ("autotune", C.c_int)]
 
 
 _u64p = C.POINTER(C.c_uint64)
@@ -91,6 +92,8 @@ ABI = [
     ("ab_write_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
     ("ab_synchronize", [C.c_void_p], C.c_int),
     ("ab_square_mul_bits", [C.c_void_p, _u64p, C.c_size_t, C.c_int32], C.c_int),
+    ("ab_set_geometry", [C.c_void_p, C.c_int], C.c_int),
+    ("ab_get_geometry", [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     ("ab_timer_start", [C.c_void_p], C.c_int),
     ("ab_timer_stop", [C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     ("ab_last_error", [], C.c_char_p),
@@ -112,6 +115,7 @@ ABI = [
     ("ab_batch_steps", [C.c_void_p, C.c_int, _u32p, _u8p], C.c_int),
     ("ab_batch_gl_mul", [C.c_void_p, C.c_int], C.c_int),
     ("ab_batch_set_geometry", [C.c_void_p, C.c_int], C.c_int),
+    ("ab_batch_autotune", [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)], C.c_int),
     ("ab_batch_synchronize", [C.c_void_p], C.c_int),
     ("ab_batch_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
     ("ab_runner_options_default", [C.POINTER(RunnerOptions)], None),
@@ -240,8 +244,18 @@ class Transform:
 
     def square_mul_bits(self, bits, count, a):
         """count squarings; step i multiplies by a when bit i of `bits` (an int) is set."""
+        bits &= (1 << count) - 1
         words = np.frombuffer(bits.to_bytes(max(8, (count + 63) // 64 * 8), "little"), dtype=np.uint64).copy()
         _check(self.L.ab_square_mul_bits(self.h, words.ctypes.data_as(_u64p), count, a))
+
+    def set_geometry(self, row_levels):
+        _check(self.L.ab_set_geometry(self.h, row_levels))
+
+    def geometry(self):
+        """(row levels, column levels) of the NTT split."""
+        rl, cl = C.c_int(), C.c_int()
+        _check(self.L.ab_get_geometry(self.h, C.byref(rl), C.byref(cl)))
+        return rl.value, cl.value
 
     def mul(self, dst, src):
         _check(self.L.ab_mul(self.h, dst, src))
@@ -423,6 +437,12 @@ class Batch:
     def set_geometry(self, lb):
         _check(self.L.ab_batch_set_geometry(self.h, lb))
 
+    def autotune(self, src, steps):
+        """Fastest row/column split for this class (times every split on copies of slot src)."""
+        lb = C.c_int()
+        _check(self.L.ab_batch_autotune(self.h, src, steps, C.byref(lb)))
+        return lb.value
+
     def synchronize(self):
         _check(self.L.ab_batch_synchronize(self.h))
 
@@ -435,11 +455,12 @@ class Batch:
 class Runner:
     """Continuous-batching PRP runner: submit tests, advance, poll results."""
 
-    def __init__(self, device=0, hbm_budget_bytes=32 << 30, max_slots_per_class=256, chunk=64):
+    def __init__(self, device=0, hbm_budget_bytes=32 << 30, max_slots_per_class=256, chunk=64, autotune=True):
         self.L = lib()
         o = RunnerOptions()
         self.L.ab_runner_options_default(C.byref(o))
         o.device, o.hbm_budget_bytes, o.max_slots_per_class, o.chunk = device, hbm_budget_bytes, max_slots_per_class, chunk
+        o.autotune = int(bool(autotune))
         h = C.c_void_p()
         _check(self.L.ab_runner_create(C.byref(o), C.byref(h)))
         self.h = h

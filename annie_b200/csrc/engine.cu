@@ -12,7 +12,9 @@
 #include <string>
 #include <vector>
 #include <stdexcept>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <cuda_runtime.h>
 
 #include "gmp.h"
@@ -180,12 +182,25 @@ struct ab_transform
 	u32 * bufp[NBUF] = {};   // device buffers (a batch slot view points into its batch)
 	bool view = false;       // true: memory and streams belong to a batch
 
+	// runs of squarings replayed from a captured CUDA graph: GRAPH_STEPS
+	// squarings whose multipliers are read from d_mult, uploaded from
+	// page-locked staging (two buffers, each reused once its upload is done)
+	static const int GRAPH_STEPS = 64;
+	cudaGraphExec_t gexec = nullptr;
+	u32 * d_mult = nullptr;
+	u32 * h_mult[2] = {};
+	cudaEvent_t mult_done[2] = {};
+	int mult_i = 0;
+
 	u32 * b(int i) const { return bufp[i]; }
 
 	~ab_transform()
 	{
 		if (view) { mpz_clears(N, factor, nullptr); return; }
 		for (cudaEvent_t e : prof) cudaEventDestroy(e);
+		if (gexec) cudaGraphExecDestroy(gexec);
+		if (d_mult) cudaFree(d_mult);
+		for (int i = 0; i < 2; ++i) { if (h_mult[i]) cudaFreeHost(h_mult[i]); if (mult_done[i]) cudaEventDestroy(mult_done[i]); }
 		if (flush_buf) cudaFree(flush_buf);
 		if (dmem) cudaFree(dmem);
 		if (ev0) cudaEventDestroy(ev0);
@@ -356,12 +371,13 @@ struct ab_transform
 	// carry(x y mod R) into AR1.  AQ0/AR0 hold the first forward levels of x;
 	// xq/xr the full forward images of y (nullptr: y = x, square).  With
 	// overlap, the Q chain runs on st2 (T_Q is only needed by the final
-	// carry-sub) and reduce_tail joins it.
-	void first_product(u32 a, const u32 * xq, const u32 * xr)
+	// carry-sub) and reduce_tail joins it.  A non-null `mult` is a device word
+	// read in place of `a` (graph replays).
+	void first_product(u32 a, const u32 * xq, const u32 * xr, const u32 * mult = nullptr)
 	{
 		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, b(WQ), xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, b(WR), xr);
-		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ);
-		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR));
+		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.mult = mult;
+		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR)); jr.mult = mult;
 		if (overlap)
 		{
 			CK(cudaEventRecord(ev_fork, st));
@@ -386,6 +402,73 @@ struct ab_transform
 		first_product(a, nullptr, nullptr);
 		reduce_tail(b(TQ), b(REG0), true, overlap);
 		prefwd = true;
+	}
+
+	// GRAPH_STEPS squarings with multipliers mults[0..GRAPH_STEPS) from the graph
+	void square_mul_graph(const u32 * mults)
+	{
+		const int G = GRAPH_STEPS;
+		if (d_mult == nullptr)
+		{
+			CK(cudaMalloc(&d_mult, G * sizeof(u32)));
+			for (int i = 0; i < 2; ++i)
+			{
+				CK(cudaMallocHost(&h_mult[i], G * sizeof(u32)));
+				CK(cudaEventCreateWithFlags(&mult_done[i], cudaEventDisableTiming));
+				CK(cudaEventRecord(mult_done[i], st));
+			}
+		}
+		if (gexec == nullptr)
+		{
+			RowJobs rjs{}; ColJobs cjs{};
+			CK(launch_rowpass(geo, tc, rjs, 1, st, 0));     // kernel attributes, outside the capture
+			CK(launch_colpass(geo, tc, cjs, 1, st, 0));
+			const uint64_t l0 = launches;
+			cudaGraph_t g = nullptr;
+			CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+			try
+			{
+				for (int s = 0; s < G; ++s)
+				{
+					first_product(1, nullptr, nullptr, d_mult + s);
+					reduce_tail(b(TQ), b(REG0), true, overlap);
+				}
+			}
+			catch (...) { cudaStreamEndCapture(st, &g); if (g) cudaGraphDestroy(g); launches = l0; throw; }
+			CK(cudaStreamEndCapture(st, &g));
+			launches = l0;
+			const cudaError_t ei = cudaGraphInstantiate(&gexec, g, 0);
+			cudaGraphDestroy(g);
+			CK(ei);
+		}
+		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		const int hi = mult_i;
+		CK(cudaEventSynchronize(mult_done[hi]));
+		std::memcpy(h_mult[hi], mults, G * sizeof(u32));
+		CK(cudaMemcpyAsync(d_mult, h_mult[hi], G * sizeof(u32), cudaMemcpyHostToDevice, st));
+		CK(cudaEventRecord(mult_done[hi], st));
+		mult_i ^= 1;
+		CK(cudaGraphLaunch(gexec, st));
+		launches += 6 * (uint64_t)G;
+		prefwd = true;
+	}
+
+	// the split and the launch constants that describe it, always together
+	void use_geometry(const Geometry & g)
+	{
+		geo = g;
+		tc.R = g.R; tc.H = g.H; tc.LA = g.LA; tc.LB = g.LB;
+	}
+
+	// row/column split of the transform (the register layouts do not depend on it)
+	void set_geometry(int lb)
+	{
+		Geometry g;
+		if (!make_geometry(prm.ln, lb, g)) throw ab_error(AB_E_ARG, "geometry not available for this length");
+		CK(cudaStreamSynchronize(st));
+		use_geometry(g);
+		prefwd = false;                          // AQ0/AR0 hold levels of the old split
+		if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
 	}
 
 	// mulMMGW (transformGPU.h:540-554)
@@ -726,7 +809,38 @@ int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, in
 {
 	return guarded([&] {
 		need_ready(h);
-		for (size_t i = 0; i < count; ++i) h->square_mul(((bits[i / 64] >> (i % 64)) & 1) ? (u32)a : 1u);
+		if (a < 1 || (count != 0 && bits == nullptr)) throw ab_error(AB_E_ARG, "bad arguments");
+		auto m_at = [&](size_t i) { return ((bits[i / 64] >> (i % 64)) & 1) ? (u32)a : 1u; };
+		size_t i = 0;
+		const size_t G = ab_transform::GRAPH_STEPS;
+		if (!h->view && h->prof_used >= h->prof.size())
+		{
+			u32 m[ab_transform::GRAPH_STEPS];
+			for (; i + G <= count; i += G)
+			{
+				for (size_t s = 0; s < G; ++s) m[s] = m_at(i + s);
+				h->square_mul_graph(m);
+			}
+		}
+		for (; i < count; ++i) h->square_mul(m_at(i));
+	});
+}
+
+int ab_set_geometry(ab_transform * h, int row_levels)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (h->view) throw ab_error(AB_E_ARG, "a batch slot takes the geometry of its batch");
+		h->set_geometry(row_levels);
+	});
+}
+
+int ab_get_geometry(const ab_transform * h, int * row_levels, int * col_levels)
+{
+	return guarded([&] {
+		if (h == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		if (row_levels) *row_levels = h->geo.LB;
+		if (col_levels) *col_levels = h->geo.LA;
 	});
 }
 
@@ -1029,7 +1143,8 @@ int ab_batch_load(ab_batch * b, int slot, const uint64_t * Nl, size_t nlimbs, in
 			if (!v->failed && (v->prm.K != b->cls.K || v->prm.pck != b->cls.pck || v->prm.ln != b->cls.ln))
 				throw ab_error(AB_E_ARG, "N does not belong to this size class");
 			if (init_failed) *init_failed = v->failed ? 1 : 0;
-			v->device = b->device; v->st = b->st; v->overlap = false; v->geo = b->geo;
+			v->device = b->device; v->st = b->st; v->overlap = false;
+			v->use_geometry(b->geo);             // the batch's split, which the autotuner may have changed
 			for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
 			v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
 			v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
@@ -1159,11 +1274,81 @@ int ab_batch_set_geometry(ab_batch * b, int lb)
 		CK(cudaStreamSynchronize(b->st));
 		b->geo = g;
 		b->tc.R = g.R; b->tc.H = g.H; b->tc.LA = g.LA; b->tc.LB = g.LB;
-		for (ab_transform * v : b->views) if (v) { v->geo = g; v->tc.R = g.R; v->tc.H = g.H; v->tc.LA = g.LA; v->tc.LB = g.LB; }
+		for (ab_transform * v : b->views) if (v) { v->use_geometry(g); v->prefwd = false; }
 		RowJobs rjs{}; ColJobs cjs{};
 		CK(launch_rowpass(b->geo, b->tc, rjs, 1, b->st, 0));
 		CK(launch_colpass(b->geo, b->tc, cjs, 1, b->st, 0));
 		if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+	});
+}
+
+// Splits chosen by ab_batch_autotune in this process, by (K, ln, capacity).
+namespace
+{
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tuned;
+
+void ok_or_throw(int rc) { if (rc != AB_OK) throw ab_error(rc, ab_last_error()); }
+}
+
+int ab_batch_autotune(ab_batch * b, int src, int steps, int * row_levels)
+{
+	return guarded([&] {
+		if (b == nullptr || src < 0 || src >= b->cap || b->views[src] == nullptr || b->views[src]->failed || steps < 1 || steps > b->max_steps)
+			throw ab_error(AB_E_ARG, "bad arguments");
+		const auto key = std::make_tuple(b->cls.K, b->cls.ln, b->cap);
+		int best = 0;
+		{
+			std::lock_guard<std::mutex> lock(g_tune_mu);
+			auto it = g_tuned.find(key);
+			if (it != g_tuned.end()) best = it->second;
+		}
+		if (best == 0)
+		{
+			// copies of `src` fill the empty slots; only they step (src and the
+			// other loaded slots keep their registers)
+			std::vector<int> tmp;
+			for (int c = 0; c < b->cap; ++c) if (b->views[c] == nullptr) { ok_or_throw(ab_batch_clone(b, c, src)); tmp.push_back(c); }
+			std::vector<u32> mult((size_t)steps * b->cap, 0u);
+			for (int s = 0; s < steps; ++s) for (int c : tmp) mult[(size_t)s * b->cap + c] = 1u;
+			cudaEvent_t e0 = nullptr, e1 = nullptr;
+			float best_ms = 0;
+			try
+			{
+				CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+				const int L = b->cls.ln - 1;
+				for (int lb = 4; lb <= 13 && !tmp.empty(); ++lb)
+				{
+					Geometry g;
+					if (!make_geometry(b->cls.ln, lb, g) || L - lb > 6) continue;
+					ok_or_throw(ab_batch_set_geometry(b, lb));
+					ok_or_throw(ab_batch_steps(b, steps, mult.data(), nullptr));     // capture and warm-up
+					CK(cudaEventRecord(e0, b->st));
+					for (int r = 0; r < 2; ++r) ok_or_throw(ab_batch_steps(b, steps, mult.data(), nullptr));
+					CK(cudaEventRecord(e1, b->st));
+					CK(cudaEventSynchronize(e1));
+					float ms = 0; CK(cudaEventElapsedTime(&ms, e0, e1));
+					if (best == 0 || ms < best_ms) { best = lb; best_ms = ms; }
+				}
+			}
+			catch (...)
+			{
+				for (int c : tmp) ab_batch_release(b, c);
+				if (e0) cudaEventDestroy(e0);
+				if (e1) cudaEventDestroy(e1);
+				throw;
+			}
+			for (int c : tmp) ok_or_throw(ab_batch_release(b, c));
+			cudaEventDestroy(e0); cudaEventDestroy(e1);
+			if (best == 0) best = b->geo.LB;      // batch full: keep the current split
+			else
+			{
+				std::lock_guard<std::mutex> lock(g_tune_mu);
+				g_tuned[key] = best;
+			}
+		}
+		if (best != b->geo.LB) ok_or_throw(ab_batch_set_geometry(b, best));
+		if (row_levels) *row_levels = best;
 	});
 }
 

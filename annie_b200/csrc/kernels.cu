@@ -705,9 +705,13 @@ bool make_geometry(int ln, int lb_override, Geometry & g)
 {
 	if (ln < 6 || ln > 20) return false;
 	const int L = ln - 1;
-	int LB = (lb_override > 0) ? lb_override : ((L - 1 < 12) ? L - 1 : 12);
-	if (L - LB > 6) LB = L - 6;
-	if (LB < 4 || LB > 13 || LB > L - 1) return false;
+	// default split, measured on B200 for single transforms (us per squaring
+	// over every split, ln 9..19): the row pass gets L - 2 levels up to 2^12
+	// points, then 11 levels, and the column pass takes the rest (at most 6)
+	static const int DEFAULT_LB[21] = {0, 0, 0, 0, 0, 0, 4, 4, 5, 6, 7, 8, 9, 10, 10, 11, 11, 11, 11, 12, 13};
+	int LB = (lb_override > 0) ? lb_override : DEFAULT_LB[ln];
+	if (lb_override <= 0 && L - LB > 6) LB = L - 6;
+	if (LB < 4 || LB > 13 || LB > L - 1 || L - LB > 6) return false;
 	g.ln = ln; g.LB = LB; g.LA = L - LB;
 	g.H = 1u << g.LA; g.R = 1u << (LB + 1); g.C = CC;
 	return true;

@@ -8,6 +8,7 @@
 // a periodic Gerbicz-Li check every `gl_check_blocks` blocks that rolls back
 // to the last verified (Reg0, Reg1) on mismatch, and host-side fault
 // injection (one register word changed between two launches).
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -63,9 +64,10 @@ int64_t gl_power(transformCUDA & t, const mpz_t res, int32_t a, int B, size_t d)
 	int64_t sq = 0;
 	const int rs = int(mpz_sizeinbase(res, 2));
 	t.set1();
-	for (int i = rs - 1; i >= B; --i) { t.square_mul(mpz_tstbit(res, (mp_bitcnt_t)i) ? a : 1); ++sq; }
+	if (rs > B) { t.square_mul_bits(res, rs - 1, rs - B, a); sq += rs - B; }
 	t.mul(transform::Reg0, d);
-	for (int i = B - 1; i >= 0; --i) { t.square_mul(((i < rs) && mpz_tstbit(res, (mp_bitcnt_t)i)) ? a : 1); ++sq; }
+	t.square_mul_bits(res, B - 1, B, a);        // bits at or above rs read as 0
+	sq += B;
 	return sq;
 }
 
@@ -199,6 +201,17 @@ int run(const mpz_t n, const ab_prp_options & o, ab_prp_result & r)
 	double last_ck = elapsed();
 	mpz_t c, e, v1, v2; mpz_inits(c, e, v1, v2, nullptr);
 
+	// runs of squarings end where something happens between two squarings: a
+	// Gerbicz-Li block boundary or the injection point; at most 4096 steps so
+	// that abort requests and checkpoint times are seen
+	auto run_end = [&](int i) {
+		int stop = std::max(0, i - 4095);
+		const int bnd = (i / B) * B;                           // largest multiple of B <= i
+		if (bnd >= stop) stop = bnd;
+		if (!injected && o.inject_iteration >= stop && o.inject_iteration <= i) stop = (int)o.inject_iteration;
+		return stop;
+	};
+
 	for (int i = i_start; i >= 0; --i)
 	{
 		if (g_quit.load(std::memory_order_relaxed))
@@ -215,8 +228,10 @@ int run(const mpz_t n, const ab_prp_options & o, ab_prp_result & r)
 			last_ck = elapsed();
 		}
 
-		t.square_mul(mpz_tstbit(E, (mp_bitcnt_t)i) ? a : 1);
-		++r.squarings;
+		const int stop = run_end(i);
+		t.square_mul_bits(E, i, (long)i - stop + 1, a);
+		r.squarings += i - stop + 1;
+		i = stop;
 
 		if (!injected && (int64_t)i == o.inject_iteration)
 		{

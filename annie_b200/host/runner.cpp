@@ -93,6 +93,7 @@ struct Class
 	std::vector<uint32_t> mult;
 	std::vector<uint8_t> snap;
 	std::vector<int> count;
+	bool tuned = false;
 };
 
 std::string hex64(uint64_t u)
@@ -220,6 +221,12 @@ struct ab_runner
 			ab_transform * v = ab_batch_slot(c->b, slot);
 			ck(ab_set1(v));
 			ck(ab_copy(v, 1, 0));
+			if (!c->tuned)
+			{
+				int lb = 0;
+				if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
+				c->tuned = true;
+			}
 			mpz_sub_ui(j->E, j->N, 1);
 			if (j->euler) mpz_fdiv_q_2exp(j->E, j->E, 1);
 			j->B = gl_block_size(mpz_sizeinbase(j->E, 2));
@@ -349,6 +356,7 @@ void ab_runner_options_default(ab_runner_options * o)
 	o->hbm_budget_bytes = (size_t)32 << 30;
 	o->max_slots_per_class = 256;
 	o->chunk = 64;
+	o->autotune = 1;
 }
 
 int ab_runner_create(const ab_runner_options * o, ab_runner ** out)

@@ -22,6 +22,7 @@ class transformCUDA : public transform
 	ab_params _p{};
 	mpz_t _N;
 	size_t _nlimbs = 0;
+	std::vector<uint64_t> _bits;
 
 	static void check(int rc)
 	{
@@ -51,6 +52,21 @@ public:
 	void set1() override { check(ab_set1(_h)); }
 	void copy(size_t dst, size_t src) override { check(ab_copy(_h, dst, src)); }
 	void square_mul(int32_t a) override { check(ab_square_mul(_h, a)); }
+
+	// `count` square_mul steps over the bits of e from bit `top` downwards:
+	// step s multiplies by a when bit top - s of e is set (one call, runs of
+	// steps replayed from a CUDA graph)
+	void square_mul_bits(const mpz_t e, long top, long count, int32_t a)
+	{
+		if (count <= 0) return;
+		_bits.assign((size_t)(count + 63) / 64, 0);
+		for (long s = 0; s < count; ++s)
+		{
+			const long bit = top - s;
+			if (bit >= 0 && mpz_tstbit(e, (mp_bitcnt_t)bit)) _bits[(size_t)s / 64] |= uint64_t(1) << (s % 64);
+		}
+		check(ab_square_mul_bits(_h, _bits.data(), (size_t)count, a));
+	}
 	void mul(size_t dst, size_t src) override { check(ab_mul(_h, dst, src)); }
 
 	void get(mpz_t & z, size_t src) override

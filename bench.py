@@ -284,31 +284,6 @@ def run_reference(args, world, rank, pg):
 # ---------------------------------------------------------------- other workloads
 SMALL_PRIMES = [p for p in range(3, 2000) if all(p % q for q in range(2, int(p ** 0.5) + 1))]
 
-def _autotune_batch(b, cls, S, mult, reps=3):
-    """Row levels per row pass for a size class: time each admissible split on the batch."""
-    ln = cls[2]
-    L = ln - 1
-    best = None
-    for lb in sorted({min(L - 1, 12), min(L - 1, 11), min(L - 1, 10), min(L - 1, 13)}):
-        if lb < 4 or lb > 13 or L - lb > 6:
-            continue
-        try:
-            b.set_geometry(lb)
-        except Exception:
-            continue
-        b.steps(mult)
-        b.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            b.steps(mult)
-        b.synchronize()
-        dt = (time.perf_counter() - t0) / reps
-        if best is None or dt < best[1]:
-            best = (lb, dt)
-    b.set_geometry(best[0])
-    return best
-
-
 def run_batch_workload(args):
     """4096 Proth candidates k*2^n+1 (k odd in [3, 2^20), n in [500000, 3000000], seeded):
     candidates/hour of the batched path (autotuned per size class, graph-captured
@@ -338,9 +313,9 @@ def run_batch_workload(args):
         b = A.Batch(cls + (0,), capacity=CAP, max_steps=S)
         b.load(0, N, 3)
         b.slot(0).set1()
+        lb = b.autotune(0, S)           # times every split on copies of slot 0 in the empty slots
         for s in range(1, CAP):
             b.clone(s, 0)
-        lb, _ = _autotune_batch(b, cls, S, mult)
         b.steps(mult)
         b.synchronize()
         t0 = time.perf_counter()
@@ -349,14 +324,17 @@ def run_batch_workload(args):
         b.synchronize()
         batch_rate = CAP * S * REPS / (time.perf_counter() - t0)       # squarings / s
         b.close()
+        # one at a time: the single-test path (graph-replayed runs of squarings,
+        # the measured default split for the length)
         t = A.Transform(N, 3)
         t.set1()
-        t.square_mul_bits(0, S, 3)
+        S1 = 256
+        t.square_mul_bits(0, S1, 3)
         t.synchronize()
         t.timer_start()
         for _ in range(REPS):
-            t.square_mul_bits(0, S, 3)
-        single_rate = S * REPS / (t.timer_stop() * 1e-3)
+            t.square_mul_bits(0, S1, 3)
+        single_rate = S1 * REPS / (t.timer_stop() * 1e-3)
         t.close()
         squarings = sum(n + k.bit_length() - 1 for k, n in members)
         t_batch += squarings / batch_rate
@@ -497,9 +475,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="square33M", choices=["square33M", "proth2M", "batch", "serve"])
     ap.add_argument("--batch-slots", type=int, default=64)
-    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.5, 2.0])
-    ap.add_argument("--serve-bits", type=int, nargs=2, default=[20000, 200000])
-    ap.add_argument("--serve-window", type=float, default=20.0)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.1, 0.4])
+    ap.add_argument("--serve-bits", type=int, nargs=2, default=[100000, 400000])
+    ap.add_argument("--serve-window", type=float, default=40.0)
     args = ap.parse_args()
     if args.workload != "square33M":
         fn = {"proth2M": run_proth2m_workload, "batch": run_batch_workload, "serve": run_serve_workload}[args.workload]

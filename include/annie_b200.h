@@ -88,8 +88,19 @@ int ab_synchronize(ab_transform * h);
 
 /* Runs `count` square_mul steps whose multipliers are `a` where the bit of
    `bits` (LSB first, bit i for step i) is set and 1 elsewhere -- the inner
-   loop of annie::check (annie.h:319-341) without the Gerbicz-Li product. */
+   loop of annie::check (annie.h:319-341) without the Gerbicz-Li product.
+   Full runs of 64 steps replay a captured CUDA graph (one launch instead of
+   384); the rest are launched one by one. */
 int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, int32_t a);
+
+/* Row/column split of the NTT: `row_levels` radix-2 levels in the row pass,
+   the other ln-1-row_levels in the column pass (at most 6).  Register
+   contents are kept.  The reference fixes its split per length at compile
+   time (transformGPU.h:403-470, forward/backward kernel choice); here it is
+   a run-time choice for the autotuner.  AB_E_ARG if the split is not
+   available for the length. */
+int ab_set_geometry(ab_transform * h, int row_levels);
+int ab_get_geometry(const ab_transform * h, int * row_levels, int * col_levels);
 
 /* Device time of the work queued since the last call, in milliseconds
    (CUDA events on the handle's stream). */

@@ -46,6 +46,12 @@ int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t
 int ab_batch_gl_mul(ab_batch * b, int slot);
 /* Row levels per row pass (0 = default split); used by the autotuner. */
 int ab_batch_set_geometry(ab_batch * b, int lb);
+/* Autotuner: times `steps` batched squarings for every admissible row/column
+   split of the class, with copies of slot `src` in the empty slots (released
+   afterwards; the loaded slots are not touched), keeps the fastest split and
+   remembers it for the process by (K, ln, capacity).  The reference picks its
+   kernel split per length at compile time (transformGPU.h:403-470). */
+int ab_batch_autotune(ab_batch * b, int src, int steps, int * row_levels);
 int ab_batch_synchronize(ab_batch * b);
 int ab_batch_launch_count(const ab_batch * b, uint64_t * count);
 
@@ -57,6 +63,7 @@ typedef struct
 	size_t hbm_budget_bytes;   /* device memory the runner may give to batches */
 	int max_slots_per_class;
 	int chunk;                 /* squarings per graph launch */
+	int autotune;              /* 1: tune the split of each new size class (ab_batch_autotune) */
 } ab_runner_options;
 
 void ab_runner_options_default(ab_runner_options * o);

@@ -125,3 +125,39 @@ def test_runner_decides_trivial_cases():
     res = _run_all(r, limit=10)
     assert res[1]["decided_early"] == 1 and res[1]["is_prp"] == 1
     assert res[2]["decided_early"] == 1 and "even" in res[2]["message"]
+
+
+def test_autotune_keeps_loaded_slots_and_results():
+    cls = (5, 4, 12)
+    nums = _same_class_numbers(cls, 3, 200000, 280000, 6)
+    b = A.Batch(cls + (0,), capacity=4, max_steps=8)
+    singles = []
+
+    def load(s, N):
+        assert not b.load(s, N, 3)
+        v = b.slot(s)
+        v.set1(); v.copy(1, 0)
+        v.square_mul(3)
+        t = A.Transform(N, 3)
+        t.set1(); t.copy(1, 0); t.square_mul(3)
+        singles.append(t)
+
+    for s in range(2):
+        load(s, nums[s][0])
+    before = [b.slot(s).read_register(0) for s in range(2)]
+    lb = b.autotune(0, 8)
+    L = cls[2] - 1
+    assert 4 <= lb <= min(13, L - 1) and L - lb <= 6
+    assert b.slot(2) is None and b.slot(3) is None          # the copies are gone
+    for s in range(2):
+        assert np.array_equal(b.slot(s).read_register(0), before[s])
+    load(2, nums[2][0])                                     # a slot loaded under the tuned split
+    mult = np.array([[3, 1, 3, 0]] * 8, dtype=np.uint32)
+    b.steps(mult)
+    for s, t in enumerate(singles):
+        for i in range(8):
+            t.square_mul(int(mult[i, s]))
+        assert np.array_equal(b.slot(s).read_register(0), t.read_register(0)), "slot %d" % s
+    b.slot(2).mul(1, 0); singles[2].mul(1, 0)
+    assert b.slot(2).get(1) == singles[2].get(1)
+    assert b.autotune(1, 8) == lb                           # remembered for the class

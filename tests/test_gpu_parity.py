@@ -149,3 +149,43 @@ def test_checkpoint_round_trip(oracle_mod):
     assert np.array_equal(t.read_register(0), t2.read_register(0))
     # a payload of another size is refused (transformGPU.h:613-616)
     assert not t2.read_checkpoint(payload[:4] + (12345).to_bytes(4, "little") + payload[8:])
+
+
+@pytest.mark.parametrize("K,ln,lbase", [(5, 12, 18), (3, 11, 21), (5, 15, 17)])
+def test_graph_runs_equal_single_steps(oracle_mod, K, ln, lbase):
+    # 2 full graph runs of 64 squarings and a remainder of 9 launched one by
+    # one, against the oracle stepping the same multipliers
+    t, o = _pair(oracle_mod, K, ln, lbase, seed=8)
+    t.set1(); o.set1()
+    count = 2 * 64 + 9
+    bits = int.from_bytes(np.random.default_rng(ln).bytes(24), "little") & ((1 << count) - 1)
+    t.square_mul_bits(bits, count, 3)
+    for i in range(count):
+        o.square_mul(3 if (bits >> i) & 1 else 1)
+    assert np.array_equal(t.read_register(0), o.read_reg(0))
+    # and once more: the graph is replayed with new multipliers
+    t.square_mul_bits(bits >> 3, 64, 3)
+    for i in range(64):
+        o.square_mul(3 if (bits >> (i + 3)) & 1 else 1)
+    assert np.array_equal(t.read_register(0), o.read_reg(0))
+    assert t.get(0) == o.get(0)
+
+
+@pytest.mark.parametrize("K,ln,lbase", [(5, 13, 17), (4, 16, 27), (5, 19, 17)])
+def test_every_geometry_gives_the_same_registers(oracle_mod, K, ln, lbase):
+    t, o = _pair(oracle_mod, K, ln, lbase, seed=4)
+    L = ln - 1
+    splits = [lb for lb in range(4, 14) if lb <= L - 1 and L - lb <= 6]
+    assert len(splits) >= 1
+    t.set1(); o.set1()
+    t.copy(1, 0); o.copy(1, 0)
+    for lb in splits:
+        t.set_geometry(lb)
+        assert t.geometry() == (lb, L - lb)
+        for a in (3, 1):
+            t.square_mul(a); o.square_mul(a)
+        t.mul(1, 0); o.mul(1, 0)
+        assert np.array_equal(t.read_register(0), o.read_reg(0)), "Reg0 differs with %d row levels" % lb
+        assert np.array_equal(t.read_register(1), o.read_reg(1)), "Reg1 differs with %d row levels" % lb
+    with pytest.raises(RuntimeError):
+        t.set_geometry(L + 5)
