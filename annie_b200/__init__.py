@@ -109,6 +109,8 @@ ABI = [
     ("ab_batch_create", [C.c_int, C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     ("ab_batch_destroy", [C.c_void_p], None),
     ("ab_batch_load", [C.c_void_p, C.c_int, _u64p, C.c_size_t, C.c_int32, C.POINTER(C.c_int)], C.c_int),
+    ("ab_batch_load_many", [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(C.c_size_t),
+                            C.POINTER(C.c_int32), C.POINTER(C.c_int)], C.c_int),
     ("ab_batch_slot", [C.c_void_p, C.c_int], C.c_void_p),
     ("ab_batch_clone", [C.c_void_p, C.c_int, C.c_int], C.c_int),
     ("ab_batch_release", [C.c_void_p, C.c_int], C.c_int),
@@ -123,6 +125,7 @@ ABI = [
     ("ab_runner_destroy", [C.c_void_p], None),
     ("ab_runner_submit", [C.c_void_p, _u64p, C.c_size_t, C.c_int, C.c_int32, C.c_uint64], C.c_int),
     ("ab_runner_advance", [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    ("ab_runner_synchronize", [C.c_void_p], C.c_int),
     ("ab_runner_poll", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(PrpResult)], C.c_int),
     ("ab_runner_stats", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_int)], C.c_int),
     ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
@@ -413,6 +416,21 @@ class Batch:
         self.Ns[slot], self.bases[slot] = N, a
         return bool(failed.value)
 
+    def load_many(self, items):
+        """items: list of (slot, N, a); loads them together (host set-up on threads).
+        Returns the init_failed flags."""
+        cnt = len(items)
+        limbs = [int_to_limbs(N) for _, N, _ in items]
+        slots = (C.c_int * cnt)(*[s for s, _, _ in items])
+        ptrs = (_u64p * cnt)(*[x.ctypes.data_as(_u64p) for x in limbs])
+        nn = (C.c_size_t * cnt)(*[len(x) for x in limbs])
+        aa = (C.c_int32 * cnt)(*[a for _, _, a in items])
+        failed = (C.c_int * cnt)()
+        _check(self.L.ab_batch_load_many(self.h, cnt, slots, ptrs, nn, aa, failed))
+        for s, N, a in items:
+            self.Ns[s], self.bases[s] = N, a
+        return [bool(f) for f in failed]
+
     def slot(self, slot):
         hv = self.L.ab_batch_slot(self.h, slot)
         return None if not hv else SlotView(self, slot, hv)
@@ -492,6 +510,9 @@ class Runner:
         while self.L.ab_runner_poll(self.h, C.byref(tag), C.byref(r)):
             out.append((tag.value, r.asdict()))
         return out
+
+    def synchronize(self):
+        _check(self.L.ab_runner_synchronize(self.h))
 
     def stats(self):
         s, l, b = C.c_uint64(), C.c_uint64(), C.c_int()

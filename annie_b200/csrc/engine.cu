@@ -12,7 +12,11 @@
 #include <string>
 #include <vector>
 #include <stdexcept>
+#include <algorithm>
+#include <atomic>
 #include <map>
+#include <memory>
+#include <thread>
 #include <mutex>
 #include <tuple>
 #include <cuda_runtime.h>
@@ -20,6 +24,7 @@
 #include "gmp.h"
 #include "kernels.h"
 #include "../../include/annie_b200.h"
+#include "../../include/annie_b200_batch.h"
 
 using namespace ab;
 
@@ -165,6 +170,7 @@ struct ab_transform
 	cudaStream_t st2 = nullptr;          // Q-domain chain, joined before the carry-sub
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_q = nullptr;
 	bool overlap = true;                 // run the Q chain on st2 (off for per-launch profiling)
+	bool split = false;                  // without overlap: still one launch per domain
 	ab_params prm{};
 	size_t n = 0;
 	Geometry geo{};
@@ -193,6 +199,10 @@ struct ab_transform
 	int mult_i = 0;
 
 	u32 * b(int i) const { return bufp[i]; }
+
+	ab_transform() { mpz_inits(N, factor, nullptr); }
+	ab_transform(const ab_transform &) = delete;
+	ab_transform & operator=(const ab_transform &) = delete;
 
 	~ab_transform()
 	{
@@ -388,6 +398,11 @@ struct ab_transform
 			rows(rr);
 			cols(jr);
 		}
+		else if (split)
+		{
+			// the launches of the overlapped schedule, in order on one stream
+			rows(rq); cols(jq); rows(rr); cols(jr);
+		}
 		else
 		{
 			rows(rq, &rr);
@@ -524,7 +539,6 @@ struct ab_transform
 
 	void prepare(const mpz_t Nin, int32_t a, const ab_params * forced, Prepared & pp)
 	{
-		mpz_inits(N, factor, nullptr);
 		mpz_set(N, Nin);
 		prm = forced ? *forced : select_params(N, a);
 		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31)
@@ -979,8 +993,11 @@ int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * co
 		h->prof_used = 0;                    // mark() records before every launch
 		const bool ov = h->overlap;
 		h->overlap = false;                  // one stream: launches in order
-		h->square_mul((u32)a);
+		h->split = true;                     // the same launches as the overlapped schedule
+		try { h->square_mul((u32)a); }
+		catch (...) { h->overlap = ov; h->split = false; throw; }
 		h->overlap = ov;
+		h->split = false;
 		const size_t used = h->prof_used;
 		h->prof_used = h->prof.size();       // recording off
 		if (used == 0 || used > (size_t)cap) throw ab_error(AB_E_CAPACITY, "launch count exceeds cap");
@@ -1111,7 +1128,6 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 		probe_t.prm = *cls; probe_t.prm.lbase = 17; probe_t.n = b->n; probe_t.geo = b->geo;
 		probe_t.build_consts();
 		b->tc = probe_t.tc;
-		mpz_inits(probe_t.N, probe_t.factor, nullptr);
 		probe_t.view = true;
 		// kernel attributes before any capture
 		RowJobs rjs{}; ColJobs cjs{};
@@ -1126,41 +1142,94 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 
 void ab_batch_destroy(ab_batch * b) { delete b; }
 
-int ab_batch_load(ab_batch * b, int slot, const uint64_t * Nl, size_t nlimbs, int32_t a, int * init_failed)
+namespace
 {
-	return guarded([&] {
-		if (b == nullptr || slot < 0 || slot >= b->cap || Nl == nullptr || nlimbs == 0 || a < 1) throw ab_error(AB_E_ARG, "bad arguments");
-		delete b->views[slot];
-		b->views[slot] = nullptr;
-		ab_transform * v = new ab_transform();
+// Host part of loading slots: parameters, R, N^-1 mod R (a gcd-sized GMP
+// computation of a few hundred ms at millions of bits) and the register
+// words, for several candidates at once on host threads.
+void batch_prepare(int count, const uint64_t * const * Nl, const size_t * nlimbs, const int32_t * a,
+                   std::vector<std::unique_ptr<ab_transform>> & views, std::vector<ab_transform::Prepared> & pp)
+{
+	views.clear();
+	for (int i = 0; i < count; ++i) { views.emplace_back(new ab_transform()); views.back()->view = true; }
+	pp.assign(count, ab_transform::Prepared());
+	std::vector<std::string> err(count);
+	std::vector<int> code(count, AB_OK);
+	auto work = [&](int i) {
 		try
 		{
-			mpz_t N; mpz_init(N); mpz_from_limbs(N, Nl, nlimbs);
-			ab_transform::Prepared pp;
-			v->view = true;
-			v->prepare(N, a, nullptr, pp);
+			mpz_t N; mpz_init(N); mpz_from_limbs(N, Nl[i], nlimbs[i]);
+			try { views[i]->prepare(N, a[i], nullptr, pp[i]); }
+			catch (...) { mpz_clear(N); throw; }
 			mpz_clear(N);
-			if (!v->failed && (v->prm.K != b->cls.K || v->prm.pck != b->cls.pck || v->prm.ln != b->cls.ln))
-				throw ab_error(AB_E_ARG, "N does not belong to this size class");
-			if (init_failed) *init_failed = v->failed ? 1 : 0;
-			v->device = b->device; v->st = b->st; v->overlap = false;
-			v->use_geometry(b->geo);             // the batch's split, which the autotuner may have changed
-			for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
-			v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
-			v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
-			if (!v->failed)
-			{
-				v->host.assign(b->words, 0);
-				v->setup_device(pp);
-				CandConst & c = b->h_cand[slot];
-				c.lbase = v->prm.lbase;
-				for (int k = 0; k < AB_MAXK; ++k) { c.rbase[k] = v->tc.rbase[k]; c.rbase_pck[k] = v->tc.rbase_pck[k]; }
-				CK(cudaMemcpyAsync(b->d_cand + slot, &c, sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
-				CK(cudaStreamSynchronize(b->st));
-			}
 		}
-		catch (...) { delete v; throw; }
-		b->views[slot] = v;
+		catch (const ab_error & e) { code[i] = e.code; err[i] = e.what(); }
+		catch (const std::exception & e) { code[i] = AB_E_ARG; err[i] = e.what(); }
+	};
+	const int nt = std::max(1, std::min(count, (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()))));
+	if (nt == 1) for (int i = 0; i < count; ++i) work(i);
+	else
+	{
+		std::atomic<int> next{0};
+		std::vector<std::thread> th;
+		for (int t = 0; t < nt; ++t) th.emplace_back([&] { for (int i; (i = next.fetch_add(1)) < count;) work(i); });
+		for (auto & x : th) x.join();
+	}
+	for (int i = 0; i < count; ++i) if (code[i] != AB_OK) throw ab_error(code[i], err[i]);
+}
+
+// Device part: the slot's buffers, the transforms of N and N^-1, the constants
+// of its digit size; the view then owns the slot.
+void batch_install(ab_batch * b, int slot, std::unique_ptr<ab_transform> & vp, const ab_transform::Prepared & pp)
+{
+	ab_transform * v = vp.get();
+	if (!v->failed && (v->prm.K != b->cls.K || v->prm.pck != b->cls.pck || v->prm.ln != b->cls.ln))
+		throw ab_error(AB_E_ARG, "N does not belong to this size class");
+	delete b->views[slot];
+	b->views[slot] = nullptr;
+	v->device = b->device; v->st = b->st; v->overlap = false;
+	v->use_geometry(b->geo);             // the batch's split, which the autotuner may have changed
+	for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
+	v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
+	v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
+	if (!v->failed)
+	{
+		v->host.assign(b->words, 0);
+		v->setup_device(pp);
+		CandConst & c = b->h_cand[slot];
+		c.lbase = v->prm.lbase;
+		for (int k = 0; k < AB_MAXK; ++k) { c.rbase[k] = v->tc.rbase[k]; c.rbase_pck[k] = v->tc.rbase_pck[k]; }
+		CK(cudaMemcpyAsync(b->d_cand + slot, &c, sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
+		CK(cudaStreamSynchronize(b->st));
+	}
+	b->views[slot] = vp.release();
+}
+}
+
+int ab_batch_load(ab_batch * b, int slot, const uint64_t * Nl, size_t nlimbs, int32_t a, int * init_failed)
+{
+	return ab_batch_load_many(b, 1, &slot, &Nl, &nlimbs, &a, init_failed);
+}
+
+int ab_batch_load_many(ab_batch * b, int count, const int * slots, const uint64_t * const * Nl, const size_t * nlimbs,
+                       const int32_t * a, int * init_failed)
+{
+	return guarded([&] {
+		if (b == nullptr || count < 0 || (count > 0 && (slots == nullptr || Nl == nullptr || nlimbs == nullptr || a == nullptr)))
+			throw ab_error(AB_E_ARG, "bad arguments");
+		for (int i = 0; i < count; ++i)
+		{
+			if (slots[i] < 0 || slots[i] >= b->cap || Nl[i] == nullptr || nlimbs[i] == 0 || a[i] < 1) throw ab_error(AB_E_ARG, "bad arguments");
+			for (int j = 0; j < i; ++j) if (slots[j] == slots[i]) throw ab_error(AB_E_ARG, "a slot is named twice");
+		}
+		std::vector<std::unique_ptr<ab_transform>> views;
+		std::vector<ab_transform::Prepared> pp;
+		batch_prepare(count, Nl, nlimbs, a, views, pp);
+		for (int i = 0; i < count; ++i)
+		{
+			if (init_failed) init_failed[i] = views[i]->failed ? 1 : 0;
+			batch_install(b, slots[i], views[i], pp[i]);
+		}
 	});
 }
 
@@ -1180,7 +1249,6 @@ int ab_batch_clone(ab_batch * b, int dst, int src)
 		b->views[dst] = nullptr;
 		ab_transform * v = new ab_transform();
 		v->view = true;
-		mpz_inits(v->N, v->factor, nullptr);
 		mpz_set(v->N, s->N); mpz_set(v->factor, s->factor);
 		v->prm = s->prm; v->n = s->n; v->geo = s->geo; v->tc = s->tc; v->failed = s->failed;
 		v->device = b->device; v->st = b->st; v->overlap = false;

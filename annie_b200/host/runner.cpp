@@ -184,9 +184,14 @@ struct ab_runner
 		return classes.back().get();
 	}
 
+	// Admission: classify queued tests, reserve a slot of their size class
+	// (creating the class within the HBM budget), then load each class's new
+	// slots together (host set-up on threads) and start their tests.
 	void admit()
 	{
 		std::deque<Job *> later;
+		struct Pending { Class * c; int slot; Job * j; };
+		std::vector<Pending> pend;
 		while (!queue.empty())
 		{
 			Job * j = queue.front(); queue.pop_front();
@@ -201,41 +206,63 @@ struct ab_runner
 			Class * c = class_for(p, true);
 			if (c == nullptr) { later.push_back(j); continue; }
 			const int slot = (int)(std::find(c->slots.begin(), c->slots.end(), nullptr) - c->slots.begin());
-			int failed = 0;
-			ck(ab_batch_load(c->b, slot, j->limbs.data(), j->limbs.size(), j->a, &failed));
-			if (failed)
-			{
-				ab_transform * v = ab_batch_slot(c->b, slot);
-				std::vector<uint64_t> f(j->limbs.size() + 2);
-				size_t cnt = 0;
-				ck(ab_get_factor(v, f.data(), f.size(), &cnt));
-				ab_batch_release(c->b, slot);
-				mpz_t z; mpz_init(z); mpz_import(z, cnt, -1, 8, 0, 0, f.data());
-				char * s = mpz_get_str(nullptr, 10, z);
-				char msg[256]; std::snprintf(msg, sizeof(msg), "%.200s divides N.", s);
-				free(s); mpz_clear(z);
-				j->r.decided_early = 1;
-				finish(j, 0, msg);
-				continue;
-			}
-			ab_transform * v = ab_batch_slot(c->b, slot);
-			ck(ab_set1(v));
-			ck(ab_copy(v, 1, 0));
-			if (!c->tuned)
-			{
-				int lb = 0;
-				if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
-				c->tuned = true;
-			}
-			mpz_sub_ui(j->E, j->N, 1);
-			if (j->euler) mpz_fdiv_q_2exp(j->E, j->E, 1);
-			j->B = gl_block_size(mpz_sizeinbase(j->E, 2));
-			j->r.gl_block = j->B;
-			j->i = (long)mpz_sizeinbase(j->E, 2) - 1;
-			j->ph = MAIN;
-			c->slots[slot] = j;
+			c->slots[slot] = j;                   // reserved
+			pend.push_back({c, slot, j});
 		}
 		queue.swap(later);
+
+		std::vector<Class *> order;
+		for (const Pending & q : pend) if (std::find(order.begin(), order.end(), q.c) == order.end()) order.push_back(q.c);
+		for (Class * c : order)
+		{
+			std::vector<Pending> mine;
+			for (const Pending & q : pend) if (q.c == c) mine.push_back(q);
+			const int cnt = (int)mine.size();
+			std::vector<int> slots(cnt), failed(cnt, 0);
+			std::vector<const uint64_t *> nl(cnt);
+			std::vector<size_t> nn(cnt);
+			std::vector<int32_t> aa(cnt);
+			for (int i = 0; i < cnt; ++i)
+			{
+				slots[i] = mine[i].slot; nl[i] = mine[i].j->limbs.data(); nn[i] = mine[i].j->limbs.size(); aa[i] = mine[i].j->a;
+			}
+			ck(ab_batch_load_many(c->b, cnt, slots.data(), nl.data(), nn.data(), aa.data(), failed.data()));
+			for (int i = 0; i < cnt; ++i)
+			{
+				Job * j = mine[i].j;
+				const int slot = mine[i].slot;
+				ab_transform * v = ab_batch_slot(c->b, slot);
+				if (failed[i])
+				{
+					std::vector<uint64_t> f(j->limbs.size() + 2);
+					size_t fc = 0;
+					ck(ab_get_factor(v, f.data(), f.size(), &fc));
+					ab_batch_release(c->b, slot);
+					c->slots[slot] = nullptr;
+					mpz_t z; mpz_init(z); mpz_import(z, fc, -1, 8, 0, 0, f.data());
+					char * s = mpz_get_str(nullptr, 10, z);
+					char msg[256]; std::snprintf(msg, sizeof(msg), "%.200s divides N.", s);
+					free(s); mpz_clear(z);
+					j->r.decided_early = 1;
+					finish(j, 0, msg);
+					continue;
+				}
+				ck(ab_set1(v));
+				ck(ab_copy(v, 1, 0));
+				if (!c->tuned)
+				{
+					int lb = 0;
+					if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
+					c->tuned = true;
+				}
+				mpz_sub_ui(j->E, j->N, 1);
+				if (j->euler) mpz_fdiv_q_2exp(j->E, j->E, 1);
+				j->B = gl_block_size(mpz_sizeinbase(j->E, 2));
+				j->r.gl_block = j->B;
+				j->i = (long)mpz_sizeinbase(j->E, 2) - 1;
+				j->ph = MAIN;
+			}
+		}
 	}
 
 	// host steps at the end of a phase (src/annie.h:343-403)
@@ -404,6 +431,17 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 	for (auto & c : r->classes) for (Job * j : c->slots) a += (j != nullptr);
 	if (active) *active = a;
 	if (queued) *queued = (int)r->queue.size();
+	return AB_OK;
+}
+
+int ab_runner_synchronize(ab_runner * r)
+{
+	if (r == nullptr) return AB_E_ARG;
+	for (auto & c : r->classes)
+	{
+		const int rc = ab_batch_synchronize(c->b);
+		if (rc != AB_OK) return rc;
+	}
 	return AB_OK;
 }
 

@@ -210,9 +210,10 @@ def run_ours(args, world, rank, local, pg):
     A_bytes = t.K * t.n * 4
     # launches of one squaring and their algorithmic bytes (reads + writes of
     # registers and operands, twiddle tables excluded), in units of A = K n 4
-    names = ["rowpass square Q+R", "colpass carry Q->TQ, R->fwdR", "rowpass mul Ninv (R)",
-             "colpass carry R+2 -> fwdQ", "rowpass mul N (Q)", "colpass carry-sub Q -> Reg0, fwdQ+R"]
-    units = [4, 4, 3, 2, 3, 5]
+    names = ["rowpass square (Q)", "colpass carry Q -> T_Q", "rowpass square (R)", "colpass carry R -> fwd R",
+             "rowpass mul Ninv (R)", "colpass carry R+2 -> fwd Q", "rowpass mul N (Q)",
+             "colpass carry-sub Q -> Reg0, fwd Q+R"]
+    units = [2, 2, 2, 2, 3, 2, 3, 5]
     peak, peak_kind = measured_peak()
     kernels = []
     for nm, u, ms in zip(names, units, per):
@@ -230,10 +231,12 @@ def run_ours(args, world, rank, local, pg):
         "achieved": kernels[dom]["GBps"], "peak": peak, "unit": "GB/s",
         "frac": round(kernels[dom]["GBps"] / peak, 4), "peak_source": peak_kind,
         "traffic": traffic,
-        "per_squaring": {"alg_bytes": 21 * A_bytes, "ms": round(sq_ms, 5),
-                         "GBps": round(21 * A_bytes / (sq_ms * 1e-3) / 1e9, 1),
-                         "frac": round(21 * A_bytes / (sq_ms * 1e-3) / 1e9 / peak, 4),
-                         "GBps_27A_model": round(27 * A_bytes / (sq_ms * 1e-3) / 1e9, 1)},
+        # whole squaring in the timed (graph-replayed, overlapped) schedule
+        "per_squaring": {"alg_bytes": 21 * A_bytes, "us": round(value, 3),
+                         "GBps": round(21 * A_bytes / (value * 1e-6) / 1e9, 1),
+                         "frac": round(21 * A_bytes / (value * 1e-6) / 1e9 / peak, 4),
+                         "GBps_27A_model": round(27 * A_bytes / (value * 1e-6) / 1e9, 1),
+                         "serial_launch_sum_ms": round(sq_ms, 5)},
         "kernels": kernels,
     }
 
@@ -290,28 +293,42 @@ def run_batch_workload(args):
     chunks) against the one-at-a-time CUDA path on the same B200."""
     import annie_b200 as A
     from annie_b200.synth import Xoshiro256ss, proth
+    from concurrent.futures import ThreadPoolExecutor
     rng = Xoshiro256ss(2024)
     cands = [(rng.uniform(3, 1 << 20) | 1, rng.uniform(500000, 3000001)) for _ in range(4096)]
+
+    # Euler base and size class of every candidate; those sharing a factor with R
+    # are decided by the gcd at set-up (as in the reference) and need no squaring
+    def info(kn):
+        N = proth(*kn)
+        a = _euler_base(N)
+        p, failed = A.probe(N, a)                        # the gcd runs in C, outside the GIL
+        return kn, a, p, failed
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        infos = list(ex.map(info, cands))
     classes = {}
-    for k, n in cands:
-        p, _ = A.probe(proth(k, n), 3, gcd=False)
-        classes.setdefault(p[:3], []).append((k, n))
+    for kn, a, p, failed in infos:
+        if not failed:
+            classes.setdefault(p[:3], []).append((kn[0], kn[1], a))
+    full = sum(len(m) for m in classes.values())
+    # iterations a candidate needs: the bits of E = (N-1)/2 = k 2^(n-1), the final
+    # Gerbicz-Li power (about B + log2 of the number of blocks) and Euler's extra one
+    def need(k, n):
+        eb = n - 1 + k.bit_length()
+        B = _gl_block(eb)
+        return eb + B + max(1, (eb // B).bit_length()) + 1
     CAP, S, REPS = args.batch_slots, 32, 4
     per_class = []
     t_batch = t_plain = 0.0
     for cls, members in sorted(classes.items()):
-        N = None
-        for k, n in members:
-            cand = proth(k, n)
-            if not A.probe(cand, 3)[1]:
-                N = cand
-                break
+        k0, n0, a0 = members[0]
+        N = proth(k0, n0)
         E = (N - 1) >> 1
         top = E.bit_length() - 1
         bits = [(E >> (top - i)) & 1 for i in range(S)]
-        mult = [[3 if bits[i] else 1] * CAP for i in range(S)]
+        mult = [[a0 if bits[i] else 1] * CAP for i in range(S)]
         b = A.Batch(cls + (0,), capacity=CAP, max_steps=S)
-        b.load(0, N, 3)
+        b.load(0, N, a0)
         b.slot(0).set1()
         lb = b.autotune(0, S)           # times every split on copies of slot 0 in the empty slots
         for s in range(1, CAP):
@@ -326,31 +343,65 @@ def run_batch_workload(args):
         b.close()
         # one at a time: the single-test path (graph-replayed runs of squarings,
         # the measured default split for the length)
-        t = A.Transform(N, 3)
+        t = A.Transform(N, a0)
         t.set1()
         S1 = 256
-        t.square_mul_bits(0, S1, 3)
+        t.square_mul_bits(0, S1, a0)
         t.synchronize()
         t.timer_start()
         for _ in range(REPS):
-            t.square_mul_bits(0, S1, 3)
+            t.square_mul_bits(0, S1, a0)
         single_rate = S1 * REPS / (t.timer_stop() * 1e-3)
         t.close()
-        squarings = sum(n + k.bit_length() - 1 for k, n in members)
+        squarings = sum(need(k, n) for k, n, _ in members)
         t_batch += squarings / batch_rate
         t_plain += squarings / single_rate
         per_class.append({"class": list(cls), "candidates": len(members), "row_levels": lb,
                           "batched_sq_per_s": round(batch_rate, 1), "single_us_per_sq": round(1e6 / single_rate, 2)})
-    value = len(cands) / (t_batch / 3600.0)
+    micro = len(cands) / (t_batch / 3600.0)
     plain = len(cands) / (t_plain / 3600.0)
+
+    # the runner on the whole candidate list: admission by size class and HBM
+    # budget, autotuned split per class, graph-captured chunks, Gerbicz-Li
+    # products; squarings completed in a fixed wall-clock window
+    r = A.Runner(chunk=S, max_slots_per_class=CAP, hbm_budget_bytes=args.batch_hbm_gb << 30)
+    for idx, (k, n) in enumerate(cands):
+        r.submit(proth(k, n), euler=True, tag=idx)
+    c0 = time.perf_counter()
+    active, queued = r.advance()
+    r.synchronize()
+    admit_s = time.perf_counter() - c0
+    for _ in range(2):
+        r.advance()
+    r.synchronize()
+    s0 = r.stats()["squarings"]
+    w0 = time.perf_counter()
+    while time.perf_counter() - w0 < args.batch_window:
+        r.advance()
+    r.synchronize()
+    window = time.perf_counter() - w0
+    st = r.stats()
+    done = len(r.poll())
+    r.close()
+    rate = (st["squarings"] - s0) / window
+    # candidates decided at set-up take no squaring: the list's time is the
+    # squarings of the others at the runner's rate
+    total_need = sum(need(k, n) for m in classes.values() for k, n, _ in m)
+    value = len(cands) * 3600.0 * rate / total_need
     return {"metric": "proth_candidates_per_hour_batched", "value": round(value, 3), "unit": "candidates/hour",
-            "n_gpus": 1, "steps": REPS, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic (seeded Proth candidates)",
-            "config": {"workload": "4096 Proth k*2^n+1, k odd in [3,2^20), n in [500000,3000000] (xoshiro256** seed 2024)",
-                       "slots_per_class": CAP, "squarings_per_graph": S,
-                       "method": "per size class: measured squarings/s of a full batch (autotuned row/column split) and of the "
-                                 "one-at-a-time path; total squarings of the 4096 candidates divided by each rate"},
+            "n_gpus": 1, "steps": 1, "warmup": 2, "ms_per_step": round(window * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Proth candidates)",
+            "config": {"workload": "4096 Proth k*2^n+1, k odd in [3,2^20), n in [500000,3000000] (xoshiro256** seed 2024), Euler",
+                       "slots_per_class": CAP, "squarings_per_graph": S, "hbm_budget_gb": args.batch_hbm_gb,
+                       "method": "continuous-batching runner over all 4096 candidates: squarings completed in a %.0f s "
+                                 "window after admission; the list's time = iterations the %d candidates without a factor "
+                                 "in common with R need / that rate (the other %d are decided at set-up by the gcd)"
+                                 % (args.batch_window, full, len(cands) - full)},
+            "runner": {"in_flight": active, "queued": queued, "batches": st["batches"], "admission_s": round(admit_s, 2),
+                       "squarings_per_s": round(rate, 1), "decided_or_finished_in_window": done,
+                       "full_tests_per_hour": round(full * 3600.0 * rate / total_need, 3)},
             "plain_candidates_per_hour": round(plain, 3), "speedup_vs_plain": round(value / plain, 3),
+            "microbench_candidates_per_hour": round(micro, 3),
             "classes": per_class}
 
 
@@ -432,37 +483,153 @@ def run_serve_workload(args):
             "rates": out_rates}
 
 
+def _jacobi(a, n):
+    """Jacobi symbol (a/n), n odd positive."""
+    a %= n
+    r = 1
+    while a:
+        while a % 2 == 0:
+            a //= 2
+            if n % 8 in (3, 5):
+                r = -r
+        a, n = n, a
+        if a % 4 == 3 and n % 4 == 3:
+            r = -r
+        a %= n
+    return r if n == 1 else 0
+
+
+def _euler_base(N):
+    """Smallest non-square a >= 2 with (a/N) = -1 (the PRP driver's rule)."""
+    import math
+    a = 2
+    while _jacobi(a, N) != -1:
+        a += 1
+        s = math.isqrt(a)
+        if s * s == a:
+            a += 1
+    return a
+
+
+def _gl_block(size):
+    L = 2 << ((size.bit_length() - 1) // 2)
+    return (size - 1) // L + 1
+
+
+def _chunk_sum(e, B):
+    s, mask = 0, (1 << B) - 1
+    while e:
+        s += e & mask
+        e >>= B
+    return s
+
+
+def _pack_bits(E, top, count):
+    """Bits E_top, E_(top-1), ... (count of them) packed LSB-first."""
+    lo = top - count + 1
+    w = (E >> lo) & ((1 << count) - 1) if lo >= 0 else (E & ((1 << (top + 1)) - 1)) << (-lo)
+    return int(format(w, "0%db" % count)[::-1], 2)
+
+
 def run_proth2m_workload(args):
-    """Proth k*2^2000000+1 (k seeded odd 20-bit), Euler: us per squaring over
-    steps of 512, and the cost of one periodic Gerbicz-Li verification."""
+    """Proth k*2^2000000+1 (k seeded odd 20-bit), Euler test with the Jacobi base:
+    device-timed run of 100,000 iterations of the test loop (Gerbicz-Li product every
+    B iterations included), then one Gerbicz-Li check and an injected single-word
+    error that the next check detects and rolls back."""
     import annie_b200 as A
     from annie_b200.synth import Xoshiro256ss, proth
     rng = Xoshiro256ss(11)
     while True:
         k = rng.uniform(1 << 19, 1 << 20) | 1
-        N = proth(k, 2000000)
-        if not A.probe(N, 3)[1]:
+        N = proth(k, args.proth_n)
+        a = _euler_base(N)
+        if not A.probe(N, a)[1]:
             break
-    t = A.Transform(N, 3)
+    t = A.Transform(N, a)
+    E = (N - 1) >> 1
+    B = _gl_block(E.bit_length())
+    state = {"i": E.bit_length() - 1}
+
+    def run(count):
+        """count iterations of the test loop from the current bit, the Gerbicz-Li
+        product after each B-aligned iteration (as the driver)."""
+        while count > 0:
+            i = state["i"]
+            stop = max(i - count + 1, (i // B) * B)
+            n = i - stop + 1
+            t.square_mul_bits(_pack_bits(E, i, n), n, a)
+            count -= n
+            state["i"] = stop - 1
+            if stop % B == 0 and stop // B != 0:
+                t.mul(1, 0)
+
+    def to_boundary():
+        run(state["i"] - (state["i"] // B) * B + 1)
+
+    def check():
+        """Periodic Gerbicz-Li check at the boundary just passed: d_now = d_prev^(2^B) a^C."""
+        i = state["i"] + 1
+        C = _chunk_sum(E >> i, B)
+        stash = t.save_checkpoint()
+        t.set1()
+        hi = C.bit_length()
+        if hi > B:
+            t.square_mul_bits(_pack_bits(C, hi - 1, hi - B), hi - B, a)
+        t.mul(0, 2)
+        t.square_mul_bits(_pack_bits(C, B - 1, B), B, a)
+        v1 = t.get(0)
+        t.read_checkpoint(stash)
+        return v1 == t.get(1), stash
+
+    def block_with_check():
+        """The next block with d_prev kept in Reg2, then its check."""
+        run(state["i"] - (state["i"] // B) * B)          # up to the boundary iteration
+        t.copy(2, 1)
+        run(1)                                            # boundary iteration + product
+        return check()
+
     t.set1()
     t.copy(1, 0)
-    S = 512
-    E = (N - 1) >> 1
-    for _ in range(args.warmup):
-        t.square_mul_bits(0, S, 3)
+    run(args.warmup * 512)
     t.synchronize()
-    ms = 0.0
-    for _ in range(args.steps):
-        t.flush_l2(256 << 20)
-        t.timer_start()
-        t.square_mul_bits(0, S, 3)
-        ms += t.timer_stop()
-    us = ms * 1e3 / (S * args.steps)
+    total = args.proth_squarings
+    t.flush_l2(256 << 20)
+    t.timer_start()
+    run(total)
+    ms = t.timer_stop()
+    us = ms * 1e3 / total
+    # one Gerbicz-Li check
+    to_boundary()
+    t.synchronize()
+    c0 = time.perf_counter()
+    ok, stash = block_with_check()
+    gl_ms = (time.perf_counter() - c0) * 1e3
+    # injected error: one residue word of Reg0 moves by one, mid-block
+    verified_i = state["i"]
+    c0 = time.perf_counter()
+    run(B // 2)
+    reg = t.read_register(0)
+    reg[12345 % len(reg)] = (int(reg[12345 % len(reg)]) - 1) % (1 << 32)
+    t.write_register(0, reg)
+    bad, _ = block_with_check()
+    t.read_checkpoint(stash)                              # roll back to the verified state
+    state["i"] = verified_i
+    redo, _ = block_with_check()
+    rb_ms = (time.perf_counter() - c0) * 1e3
+    blocks = total / B
     return {"metric": "us_per_squaring_proth_n2M", "value": round(us, 3), "unit": "us/squaring", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Proth number)",
-            "config": {"workload": "Proth k*2^2000000+1, k=%d, Euler test" % k, "ln": t.ln, "K": t.K, "lbase": t.lbase,
-                       "squarings_per_step": S}}
+            "steps": int(round(blocks)), "warmup": args.warmup, "ms_per_step": round(ms / blocks, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Proth number)",
+            "config": {"workload": "Proth k*2^%d+1, k=%d, Euler test base %d; %d test iterations timed "
+                                   "(one step = one Gerbicz-Li block of B=%d iterations + its product)"
+                                   % (args.proth_n, k, a, total, B),
+                       "ln": t.ln, "K": t.K, "lbase": t.lbase, "gl_block": B,
+                       "l2": "256 MiB write before the timed region; the working set (about 10 MB) stays in L2"},
+            "gl_check": {"ms": round(gl_ms, 2), "passed": bool(ok)},
+            "injected_error": {"detected": not bad, "rolled_back_and_verified": bool(redo), "ms": round(rb_ms, 2),
+                               "note": "one Reg0 word changed by one mid-block; time from the change through the failed "
+                                       "check, the reload of the verified state and the repeated, verified block"}}
 
 
 def main():
@@ -478,6 +645,10 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.1, 0.4])
     ap.add_argument("--serve-bits", type=int, nargs=2, default=[100000, 400000])
     ap.add_argument("--serve-window", type=float, default=40.0)
+    ap.add_argument("--proth-squarings", type=int, default=100000)
+    ap.add_argument("--proth-n", type=int, default=2000000)
+    ap.add_argument("--batch-window", type=float, default=30.0)
+    ap.add_argument("--batch-hbm-gb", type=int, default=16)
     args = ap.parse_args()
     if args.workload != "square33M":
         fn = {"proth2M": run_proth2m_workload, "batch": run_batch_workload, "serve": run_serve_workload}[args.workload]

@@ -113,7 +113,10 @@ const char * ab_last_error(void);
 int ab_launch_count(const ab_transform * h, uint64_t * count);
 
 /* Runs one square_mul(a) with a CUDA event before every kernel launch and
-   returns each launch's device time (ms, launch order) in ms[0..*count). */
+   returns each launch's device time (ms, launch order) in ms[0..*count).
+   The launches are those of the overlapped schedule (one per domain: row
+   and column pass of Q, of R, then the reduction), serialised on one
+   stream so that each is timed alone. */
 int ab_profile_square(ab_transform * h, int32_t a, float * ms, int cap, int * count);
 
 /* Overwrites a device buffer of `bytes` (allocated on first use) on the

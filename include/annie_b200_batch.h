@@ -33,6 +33,12 @@ void ab_batch_destroy(ab_batch * b);
 /* Sets up slot `slot` for N and base a (the digit size may differ between
    slots); N must fall in the class (K, pck, ln) by the factory rule. */
 int ab_batch_load(ab_batch * b, int slot, const uint64_t * N, size_t nlimbs, int32_t a, int * init_failed);
+/* ab_batch_load for `count` candidates at once: the host part of each load
+   (parameters, N^-1 mod R, register words) runs on host threads, then the
+   slots are set up on the device one after the other.  init_failed (nullable)
+   receives one flag per candidate. */
+int ab_batch_load_many(ab_batch * b, int count, const int * slots, const uint64_t * const * N, const size_t * nlimbs,
+                       const int32_t * a, int * init_failed);
 ab_transform * ab_batch_slot(ab_batch * b, int slot);
 /* Slot dst becomes a copy of loaded slot src (same N and base, registers
    included) without the host set-up: for re-tests and throughput runs. */
@@ -74,6 +80,8 @@ int ab_runner_submit(ab_runner * r, const uint64_t * N, size_t nlimbs, int euler
 /* Admits queued tests into free slots, then runs one chunk of every batch and
    the host steps of the tests that reached the end of a phase. */
 int ab_runner_advance(ab_runner * r, int * active, int * queued);
+/* Waits for the work queued by ab_runner_advance on every batch. */
+int ab_runner_synchronize(ab_runner * r);
 /* Pops one finished test; returns 1 if one was available, 0 otherwise. */
 int ab_runner_poll(ab_runner * r, uint64_t * tag, ab_prp_result * out);
 /* Squarings executed for tests since creation (all slots). */

@@ -161,3 +161,34 @@ def test_autotune_keeps_loaded_slots_and_results():
     b.slot(2).mul(1, 0); singles[2].mul(1, 0)
     assert b.slot(2).get(1) == singles[2].get(1)
     assert b.autotune(1, 8) == lb                           # remembered for the class
+
+
+def test_load_many_equals_single_loads():
+    cls = (5, 4, 12)
+    nums = _same_class_numbers(cls, 3, 200000, 280000, 9)
+    rng = Xoshiro256ss(10)
+    while True:                                  # a class member that shares the factor 3 with R
+        N3 = rng.random_odd(240000)
+        if N3 % 3 == 0 and A.probe(N3, 3)[0][:3] == cls:
+            break
+    b = A.Batch(cls + (0,), capacity=5, max_steps=8)
+    failed = b.load_many([(4, nums[0][0], 3), (1, nums[1][0], 3), (2, N3, 3), (0, nums[2][0], 3)])
+    assert failed == [False, False, True, False]
+    assert b.slot(2).get_factor() % 3 == 0
+    b.release(2)
+    order = [(4, nums[0][0], 3), (1, nums[1][0], 3), (0, nums[2][0], 3)]
+    singles = []
+    for s, N, a in order:
+        v = b.slot(s)
+        v.set1()
+        t = A.Transform(N, a)
+        t.set1()
+        singles.append(t)
+    mult = np.zeros((8, 5), dtype=np.uint32)
+    mult[:, 4] = 3; mult[:, 1] = 1; mult[:, 0] = 3
+    b.steps(mult)
+    for (s, N, a), t in zip(order, singles):
+        for i in range(8):
+            t.square_mul(int(mult[i, s]))
+        assert np.array_equal(b.slot(s).read_register(0), t.read_register(0)), "slot %d" % s
+        assert b.slot(s).get(0) == pow(int(mult[0, s]), 255, N)       # 8 steps of r = m r^2 from r = 1
