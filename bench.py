@@ -51,19 +51,25 @@ def dist_setup():
     return world, rank, local, pg
 
 
+def _dev(pg):
+    """Tensors for collectives live on the GPU under NCCL, on the CPU under gloo."""
+    return "cuda" if pg.get_backend() == "nccl" else "cpu"
+
+
 def barrier(pg):
     if pg is not None:
         import torch
-        t = torch.ones(1, device="cuda")
+        t = torch.ones(1, device=_dev(pg))
         pg.all_reduce(t)
-        torch.cuda.synchronize()
+        if _dev(pg) == "cuda":
+            torch.cuda.synchronize()
 
 
 def allmax(pg, value):
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -72,9 +78,14 @@ def allsum(pg, value):
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t)
     return float(t.item())
+
+
+def shard(items, rank, world):
+    """The rank's share of independent work units (candidates): every world-th item."""
+    return items[rank::world]
 
 
 def measured_peak():
@@ -287,7 +298,7 @@ def run_reference(args, world, rank, pg):
 # ---------------------------------------------------------------- other workloads
 SMALL_PRIMES = [p for p in range(3, 2000) if all(p % q for q in range(2, int(p ** 0.5) + 1))]
 
-def run_batch_workload(args):
+def run_batch_workload(args, world=1, rank=0, local=0, pg=None):
     """4096 Proth candidates k*2^n+1 (k odd in [3, 2^20), n in [500000, 3000000], seeded):
     candidates/hour of the batched path (autotuned per size class, graph-captured
     chunks) against the one-at-a-time CUDA path on the same B200."""
@@ -327,7 +338,7 @@ def run_batch_workload(args):
         top = E.bit_length() - 1
         bits = [(E >> (top - i)) & 1 for i in range(S)]
         mult = [[a0 if bits[i] else 1] * CAP for i in range(S)]
-        b = A.Batch(cls + (0,), capacity=CAP, max_steps=S)
+        b = A.Batch(cls + (0,), capacity=CAP, max_steps=S, device=local)
         b.load(0, N, a0)
         b.slot(0).set1()
         lb = b.autotune(0, S)           # times every split on copies of slot 0 in the empty slots
@@ -343,7 +354,7 @@ def run_batch_workload(args):
         b.close()
         # one at a time: the single-test path (graph-replayed runs of squarings,
         # the measured default split for the length)
-        t = A.Transform(N, a0)
+        t = A.Transform(N, a0, device=local)
         t.set1()
         S1 = 256
         t.square_mul_bits(0, S1, a0)
@@ -358,14 +369,16 @@ def run_batch_workload(args):
         t_plain += squarings / single_rate
         per_class.append({"class": list(cls), "candidates": len(members), "row_levels": lb,
                           "batched_sq_per_s": round(batch_rate, 1), "single_us_per_sq": round(1e6 / single_rate, 2)})
-    micro = len(cands) / (t_batch / 3600.0)
-    plain = len(cands) / (t_plain / 3600.0)
+    # (with several ranks, the plain path runs one test per GPU at a time)
+    micro = world * len(cands) / (t_batch / 3600.0)
+    plain = world * len(cands) / (t_plain / 3600.0)
 
     # the runner on the whole candidate list: admission by size class and HBM
     # budget, autotuned split per class, graph-captured chunks, Gerbicz-Li
     # products; squarings completed in a fixed wall-clock window
-    r = A.Runner(chunk=S, max_slots_per_class=CAP, hbm_budget_bytes=args.batch_hbm_gb << 30)
-    for idx, (k, n) in enumerate(cands):
+    # (ranks: each runs its share of the list, no data-path collective)
+    r = A.Runner(device=local, chunk=S, max_slots_per_class=CAP, hbm_budget_bytes=args.batch_hbm_gb << 30)
+    for idx, (k, n) in shard(list(enumerate(cands)), rank, world):
         r.submit(proth(k, n), euler=True, tag=idx)
     c0 = time.perf_counter()
     active, queued = r.advance()
@@ -374,16 +387,17 @@ def run_batch_workload(args):
     for _ in range(2):
         r.advance()
     r.synchronize()
+    barrier(pg)
     s0 = r.stats()["squarings"]
     w0 = time.perf_counter()
     while time.perf_counter() - w0 < args.batch_window:
         r.advance()
     r.synchronize()
-    window = time.perf_counter() - w0
+    window = allmax(pg, time.perf_counter() - w0)
     st = r.stats()
-    done = len(r.poll())
+    done = int(allsum(pg, len(r.poll())))
     r.close()
-    rate = (st["squarings"] - s0) / window
+    rate = allsum(pg, st["squarings"] - s0) / window
     # candidates decided at set-up take no squaring: the list's time is the
     # squarings of the others at the runner's rate
     total_need = sum(need(k, n) for m in classes.values() for k, n, _ in m)
@@ -650,11 +664,24 @@ def main():
     ap.add_argument("--batch-window", type=float, default=30.0)
     ap.add_argument("--batch-hbm-gb", type=int, default=16)
     args = ap.parse_args()
-    if args.workload != "square33M":
-        fn = {"proth2M": run_proth2m_workload, "batch": run_batch_workload, "serve": run_serve_workload}[args.workload]
-        print(json.dumps(fn(args)), flush=True)
-        return
     world, rank, local, pg = dist_setup()
+    if args.workload == "batch":
+        # candidates shard across ranks (each rank its own runner)
+        line = run_batch_workload(args, world, rank, local, pg)
+        line["n_gpus"] = world
+        if pg is not None:
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    if args.workload != "square33M":
+        # single-test latency workloads: one GPU (rank 0); other ranks have no work
+        if rank == 0:
+            fn = {"proth2M": run_proth2m_workload, "serve": run_serve_workload}[args.workload]
+            print(json.dumps(fn(args)), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         line = run_reference(args, world, rank, pg)
         if line is not None:
