@@ -193,6 +193,7 @@ struct ab_transform
 	// page-locked staging (two buffers, each reused once its upload is done)
 	static const int GRAPH_STEPS = 64;
 	cudaGraphExec_t gexec = nullptr;
+	uint64_t graph_kernels = 0;          // kernel nodes in gexec
 	u32 * d_mult = nullptr;
 	u32 * h_mult[2] = {};
 	cudaEvent_t mult_done[2] = {};
@@ -451,6 +452,7 @@ struct ab_transform
 			}
 			catch (...) { cudaStreamEndCapture(st, &g); if (g) cudaGraphDestroy(g); launches = l0; throw; }
 			CK(cudaStreamEndCapture(st, &g));
+			graph_kernels = launches - l0;       // counted by rows()/cols() while recording
 			launches = l0;
 			const cudaError_t ei = cudaGraphInstantiate(&gexec, g, 0);
 			cudaGraphDestroy(g);
@@ -464,7 +466,7 @@ struct ab_transform
 		CK(cudaEventRecord(mult_done[hi], st));
 		mult_i ^= 1;
 		CK(cudaGraphLaunch(gexec, st));
-		launches += 6 * (uint64_t)G;
+		launches += graph_kernels;
 		prefwd = true;
 	}
 
