@@ -196,6 +196,17 @@ __device__ __forceinline__ Big<K> big_sar(const Big<K> & a, int s)
 	return r;
 }
 
+// v as K two's-complement limbs (v fits 32K bits)
+template <int K>
+__device__ __forceinline__ Big<K> big_from_i128(__int128 v)
+{
+	Big<K> r;
+	const u32 s = (v < 0) ? 0xffffffffu : 0u;
+#pragma unroll
+	for (int i = 0; i < K; ++i) r.l[i] = (i < 4) ? (u32)((unsigned __int128)v >> (32 * i)) : s;
+	return r;
+}
+
 template <int K>
 __device__ __forceinline__ u64 big_low64(const Big<K> & a) { return (u64)a.l[0] | ((u64)a.l[1] << 32); }
 

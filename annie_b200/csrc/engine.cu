@@ -373,6 +373,7 @@ struct ab_transform
 		rows(rj(b(AQ1), ROW_MUL, b(WQ), b(NQ)));
 		if (join_q) CK(cudaStreamWaitEvent(st, ev_q, 0));
 		ColJob j2 = cj_tr(b(AQ1), b(WQ), 1, 1, tq, LOWER_Q); j2.out_norm = out;
+		j2.sub_big = (tq == b(TQ)) ? 1 : 0;     // T_Q of first_product holds exact coefficient values
 		if (want_prefwd) set_fwd(j2, b(AQ0), b(WQ), b(AR0), b(WR));
 		cols(j2);
 	}
@@ -387,7 +388,7 @@ struct ab_transform
 	void first_product(u32 a, const u32 * xq, const u32 * xr, const u32 * mult = nullptr)
 	{
 		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, b(WQ), xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, b(WR), xr);
-		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.mult = mult;
+		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.out_big = 1; jq.mult = mult;
 		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR)); jr.mult = mult;
 		if (overlap)
 		{
@@ -680,14 +681,14 @@ struct ab_batch
 			const u32 * mult = ctrl(s, 0), * act = ctrl(s, 1), * snap = ctrl(s, 2);
 			RowJob rq = rj(aq0, ROW_SQUARE, wq, nullptr, act), rr = rj(ar0, ROW_SQUARE, wr, nullptr, act);
 			rows(rq, &rr);
-			ColJob jq = cj(aq0, true, wq, mult, 1, nullptr, LOWER_NONE); jq.out_norm = base[T::TQ];
+			ColJob jq = cj(aq0, true, wq, mult, 1, nullptr, LOWER_NONE); jq.out_norm = base[T::TQ]; jq.out_big = 1;
 			ColJob jr = cj(ar0, true, wr, mult, 0, nullptr, LOWER_NONE); jr.out_fwd[1] = ar1; jr.w_out[1] = wr;
 			cols(jq, &jr);
 			rows(rj(ar1, ROW_MUL, wr, base[T::NIR], act));
 			ColJob j1 = cj(ar1, true, wr, act, 0, nullptr, LOWER_R_ADD2); j1.out_fwd[0] = aq1; j1.w_out[0] = wq;
 			cols(j1);
 			rows(rj(aq1, ROW_MUL, wq, base[T::NQ], act));
-			ColJob j2 = cj(aq1, true, wq, act, 1, base[T::TQ], LOWER_Q);
+			ColJob j2 = cj(aq1, true, wq, act, 1, base[T::TQ], LOWER_Q); j2.sub_big = 1;
 			j2.out_norm = base[T::REG0];
 			j2.out_fwd[0] = aq0; j2.w_out[0] = wq; j2.out_fwd[1] = ar0; j2.w_out[1] = wr;
 			j2.out_snap = base[T::SNAP]; j2.snap_flag = snap;

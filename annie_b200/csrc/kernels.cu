@@ -417,10 +417,22 @@ __device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const 
 	}
 }
 
-// Second carry phase for one group of 4 coefficients: f = carry-in, d = the
-// group's unsigned digits; writes the balanced re-encoded residues and returns
-// the top sub-digit of the last coefficient (kernel.cl:1582-1613).
+// Exact value of a balanced coefficient: unsigned digits e_0 .. e_{PCK-2} and
+// the signed top digit, base 2^lb.
 template <int K, int PCK>
+__device__ __forceinline__ Big<K> digits_value(int lb, i32 top, const u32 (&e)[PCK])
+{
+	__int128 v = (__int128)top;
+#pragma unroll
+	for (int l = PCK - 2; l >= 0; --l) v = (v << lb) + (__int128)e[l];
+	return big_from_i128<K>(v);
+}
+
+// Second carry phase for one group of 4 coefficients: f = carry-in, d = the
+// group's unsigned digits; writes the balanced re-encoded residues (BIG: the
+// exact coefficient values as K limbs) and returns the top sub-digit of the
+// last coefficient (kernel.cl:1582-1613).
+template <int K, int PCK, bool BIG>
 __device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 * rbase, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
 {
 	const i32 base = (i32)(1u << lb);
@@ -432,7 +444,13 @@ __device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 
 		extract_shift<K, PCK>(f, lb, e);
 		i32 top = (i32)e[PCK - 1];
 		if (top >= base / 2) { top -= base; f = big_add_u32<K>(f, 1u); }
-		encode_digits<K, PCK>(c, rbase, top, e, res[j]);
+		if (BIG)
+		{
+			const Big<K> v = digits_value<K, PCK>(lb, top, e);
+#pragma unroll
+			for (int k = 0; k < K; ++k) res[j][k] = v.l[k];
+		}
+		else encode_digits<K, PCK>(c, rbase, top, e, res[j]);
 	}
 	f = add_digits<K, PCK>(f, lb, d[3]);
 	const u32 bm = (u32)base - 1;
@@ -458,7 +476,13 @@ __device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 
 		e[2 % PCK] = (u32)r23 & bm;
 		top = (i32)(r23 >> lb);
 	}
-	encode_digits<K, PCK>(c, rbase, top, e, res[3]);
+	if (BIG)
+	{
+		const Big<K> v = digits_value<K, PCK>(lb, top, e);
+#pragma unroll
+		for (int k = 0; k < K; ++k) res[3][k] = v.l[k];
+	}
+	else encode_digits<K, PCK>(c, rbase, top, e, res[3]);
 	return top;
 }
 
@@ -565,9 +589,19 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 				f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
 				if (J.sub != nullptr)
 				{
+					Big<K> s;
+					if (J.sub_big)
+					{
 #pragma unroll
-					for (int k = 0; k < K; ++k) rr[k] = sv[k][j];
-					f = big_sub<K>(f, garner<K>(c, rr));
+						for (int k = 0; k < K; ++k) s.l[k] = sv[k][j];
+					}
+					else
+					{
+#pragma unroll
+						for (int k = 0; k < K; ++k) rr[k] = sv[k][j];
+						s = garner<K>(c, rr);
+					}
+					f = big_sub<K>(f, s);
 				}
 				extract_shift<K, PCK>(f, lb, dg[j]);
 			}
@@ -617,7 +651,8 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 				dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
 			}
 			u32 res[4][K];
-			const i32 top = carry_phase2<K, PCK>(c, lb, cc.rbase, f, dg, res);
+			const i32 top = J.out_big ? carry_phase2<K, PCK, true>(c, lb, cc.rbase, f, dg, res)
+			                          : carry_phase2<K, PCK, false>(c, lb, cc.rbase, f, dg, res);
 			const bool is_last = (row == H - 1) && (u4 == ng - 1) && (b == nb - 1);
 			if ((is_last || !store) && top >= (i32)(1u << lb)) decision = 1;
 			if (store)

@@ -43,8 +43,11 @@ struct ColJob
 	u32 a;               // carry: multiply by a
 	int nega;            // carry: wrap-around negated (mod x^n + 1)
 	const u32 * sub;     // carry: subtract this normal-form register (nullable)
+	int sub_big;         // 1: `sub` holds exact coefficient values (K two's-complement limbs per coefficient, as out_big writes)
 	int lower;           // LowerMode applied after the carry
 	u32 * out_norm;      // normal-form result (nullable)
+	int out_big;         // 1: out_norm receives each coefficient's exact value (K limbs, plane k = limb k)
+	                     // instead of its residues -- for T_Q, which only the subtracting carry reads
 	u32 * out_fwd[2];    // first LA forward levels of the result, per domain (nullable)
 	const u32 * w_out[2];
 	size_t stride;       // words between candidates (batches)
