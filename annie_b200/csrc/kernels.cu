@@ -430,12 +430,86 @@ __device__ __forceinline__ Big<K> digits_value(int lb, i32 top, const u32 (&e)[P
 	return big_from_i128<K>(v);
 }
 
-// Second carry phase for one group of 4 coefficients: f = carry-in, d = the
-// group's unsigned digits; writes the balanced re-encoded residues (BIG: the
+// Second carry phase for one group of 4 coefficients, in place in the tile:
+// tp points at the group's first coefficient, plane l (digits) / k (residues)
+// at tp + l * PS.  f = carry-in; each coefficient's digits are replaced by its
+// balanced re-encoded residues (big: its exact value as K limbs); returns the
+// top sub-digit of the last coefficient (kernel.cl:1582-1613).  The loop is
+// rolled, so that the column pass body stays small enough for the
+// instruction cache; a coefficient's digits are read before its residues
+// overwrite them.
+template <int K, int PCK>
+__device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 * rbase, Big<K> f, u32 * tp, int PS, bool big, bool store)
+{
+	const i32 base = (i32)(1u << lb);
+	auto put = [&](int j, i32 top, const u32 (&e)[PCK]) {
+		u32 r[K];
+		if (big)
+		{
+			const Big<K> v = digits_value<K, PCK>(lb, top, e);
+#pragma unroll
+			for (int k = 0; k < K; ++k) r[k] = v.l[k];
+		}
+		else encode_digits<K, PCK>(c, rbase, top, e, r);
+		if (store)
+		{
+#pragma unroll
+			for (int k = 0; k < K; ++k) tp[k * PS + j] = r[k];
+		}
+	};
+#pragma unroll 1
+	for (int j = 0; j < 3; ++j)
+	{
+		u32 d[PCK];
+#pragma unroll
+		for (int l = 0; l < PCK; ++l) d[l] = tp[l * PS + j];
+		f = add_digits<K, PCK>(f, lb, d);
+		u32 e[PCK];
+		extract_shift<K, PCK>(f, lb, e);
+		i32 top = (i32)e[PCK - 1];
+		if (top >= base / 2) { top -= base; f = big_add_u32<K>(f, 1u); }
+		put(j, top, e);
+	}
+	{
+		u32 d[PCK];
+#pragma unroll
+		for (int l = 0; l < PCK; ++l) d[l] = tp[l * PS + 3];
+		f = add_digits<K, PCK>(f, lb, d);
+	}
+	const u32 bm = (u32)base - 1;
+	u32 e[PCK];
+	i32 top;
+	if (PCK == 1)
+	{
+		top = (i32)(i64)big_low64<K>(f);
+	}
+	else if (PCK == 2)
+	{
+		const i64 r01 = (i64)big_low64<K>(f);
+		e[0] = (u32)r01 & bm;
+		top = (i32)(r01 >> lb);
+	}
+	else
+	{
+		const u64 r01 = big_low64<K>(f) & (((u64)1 << (2 * lb)) - 1);
+		e[0] = (u32)r01 & bm;
+		e[1 % PCK] = (u32)(r01 >> lb);
+		const Big<K> f23 = big_sar<K>(f, 2 * lb);
+		const i64 r23 = (i64)big_low64<K>(f23);
+		e[2 % PCK] = (u32)r23 & bm;
+		top = (i32)(r23 >> lb);
+	}
+	put(3, top, e);
+	return top;
+}
+
+// The same second phase unrolled over the 4 coefficients (faster for tall
+// columns, LOG_H >= 5, where the body fits the instruction cache less badly
+// than the lost parallelism costs): f = carry-in, d = the group's unsigned digits; writes the balanced re-encoded residues (BIG: the
 // exact coefficient values as K limbs) and returns the top sub-digit of the
 // last coefficient (kernel.cl:1582-1613).
 template <int K, int PCK, bool BIG>
-__device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 * rbase, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
+__device__ __forceinline__ i32 carry_phase2_unrolled(const TConst & c, int lb, const u32 * rbase, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
 {
 	const i32 base = (i32)(1u << lb);
 #pragma unroll
@@ -492,6 +566,10 @@ template <int LOG_H, int K, int PCK>
 __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, const TConst c)
 {
 	constexpr int H = 1 << LOG_H;
+	// carry loops rolled over the 4 coefficients of a group for short columns,
+	// unrolled for tall ones (measured: 12 % faster at LOG_H = 3 with K = 5,
+	// equal at 4, 2 % slower at 5 and 6)
+	constexpr bool ROLL = (LOG_H <= 4);
 	extern __shared__ __align__(16) u32 sm[];
 	u32 * const tile = sm;                       // [K][H][TW]
 	u32 * const cw = tile + K * H * TW;          // [H][TW/4][K] carry-out words
@@ -562,54 +640,92 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 		{
 			const int row = idx / ng, u4 = idx % ng;
 			if (E == 8 && u4 == 0 && row != H - 1) continue;
-			u32 xv[K][4];
+			Big<K> f;
+			if constexpr (ROLL)
+			{
+				// rolled over the 4 coefficients (code size); coefficient j's digits
+				// overwrite its residues once they are read
+				u32 * const tp = tile + row * TW + 4 * u4;
+				const u32 * const sp = (J.sub != nullptr) ? J.sub + (size_t)row * R + gcol(4 * u4) : nullptr;
+				f = big_zero<K>();
+#pragma unroll 1
+				for (int j = 0; j < 4; ++j)
+				{
+					u32 rr[K];
 #pragma unroll
-			for (int k = 0; k < K; ++k)
-			{
-				const uint4 t = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + 4 * u4);
-				xv[k][0] = t.x; xv[k][1] = t.y; xv[k][2] = t.z; xv[k][3] = t.w;
+					for (int k = 0; k < K; ++k) rr[k] = mont_mul(tp[k * H * TW + j], c.norm[k], c.p[k], c.q[k]);
+					const Big<K> V = garner<K>(c, rr);
+					f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
+					if (sp != nullptr)
+					{
+#pragma unroll
+						for (int k = 0; k < K; ++k) rr[k] = __ldg(sp + (size_t)k * n + j);
+						Big<K> sv;
+						if (J.sub_big)
+						{
+#pragma unroll
+							for (int k = 0; k < K; ++k) sv.l[k] = rr[k];
+						}
+						else sv = garner<K>(c, rr);
+						f = big_sub<K>(f, sv);
+					}
+					u32 dg[PCK];
+					extract_shift<K, PCK>(f, lb, dg);
+#pragma unroll
+					for (int l = 0; l < PCK; ++l) tp[l * H * TW + j] = dg[l];
+				}
 			}
-			u32 sv[K][4];
-			if (J.sub != nullptr)
+			else
 			{
+				u32 xv[K][4];
 #pragma unroll
 				for (int k = 0; k < K; ++k)
 				{
-					const uint4 t = __ldg(reinterpret_cast<const uint4 *>(J.sub + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
-					sv[k][0] = t.x; sv[k][1] = t.y; sv[k][2] = t.z; sv[k][3] = t.w;
+					const uint4 t = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + 4 * u4);
+					xv[k][0] = t.x; xv[k][1] = t.y; xv[k][2] = t.z; xv[k][3] = t.w;
 				}
-			}
-			Big<K> f = big_zero<K>();
-			u32 dg[4][PCK];
-#pragma unroll
-			for (int j = 0; j < 4; ++j)
-			{
-				u32 rr[K];
-#pragma unroll
-				for (int k = 0; k < K; ++k) rr[k] = mont_mul(xv[k][j], c.norm[k], c.p[k], c.q[k]);
-				const Big<K> V = garner<K>(c, rr);
-				f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
+				u32 sv[K][4];
 				if (J.sub != nullptr)
 				{
-					Big<K> s;
-					if (J.sub_big)
-					{
 #pragma unroll
-						for (int k = 0; k < K; ++k) s.l[k] = sv[k][j];
-					}
-					else
+					for (int k = 0; k < K; ++k)
 					{
-#pragma unroll
-						for (int k = 0; k < K; ++k) rr[k] = sv[k][j];
-						s = garner<K>(c, rr);
+						const uint4 t = __ldg(reinterpret_cast<const uint4 *>(J.sub + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
+						sv[k][0] = t.x; sv[k][1] = t.y; sv[k][2] = t.z; sv[k][3] = t.w;
 					}
-					f = big_sub<K>(f, s);
 				}
-				extract_shift<K, PCK>(f, lb, dg[j]);
-			}
+				f = big_zero<K>();
+				u32 dg[4][PCK];
 #pragma unroll
-			for (int l = 0; l < PCK; ++l)
-				*reinterpret_cast<uint4 *>(tile + (l * H + row) * TW + 4 * u4) = make_uint4(dg[0][l], dg[1][l], dg[2][l], dg[3][l]);
+				for (int j = 0; j < 4; ++j)
+				{
+					u32 rr[K];
+#pragma unroll
+					for (int k = 0; k < K; ++k) rr[k] = mont_mul(xv[k][j], c.norm[k], c.p[k], c.q[k]);
+					const Big<K> V = garner<K>(c, rr);
+					f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
+					if (J.sub != nullptr)
+					{
+						Big<K> s;
+						if (J.sub_big)
+						{
+#pragma unroll
+							for (int k = 0; k < K; ++k) s.l[k] = sv[k][j];
+						}
+						else
+						{
+#pragma unroll
+							for (int k = 0; k < K; ++k) rr[k] = sv[k][j];
+							s = garner<K>(c, rr);
+						}
+						f = big_sub<K>(f, s);
+					}
+					extract_shift<K, PCK>(f, lb, dg[j]);
+				}
+#pragma unroll
+				for (int l = 0; l < PCK; ++l)
+					*reinterpret_cast<uint4 *>(tile + (l * H + row) * TW + 4 * u4) = make_uint4(dg[0][l], dg[1][l], dg[2][l], dg[3][l]);
+			}
 #pragma unroll
 			for (int k = 0; k < K; ++k) cw[(row * (TW / 4) + u4) * K + k] = f.l[k];
 		}
@@ -645,24 +761,30 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 #pragma unroll
 			for (int k = 0; k < K; ++k) f.l[k] = cw[(prow * (TW / 4) + pu4) * K + k];
 			if (neg) f = big_neg<K>(f);
-			u32 dg[4][PCK];
-#pragma unroll
-			for (int l = 0; l < PCK; ++l)
+			i32 top;
+			if constexpr (ROLL)
+				top = carry_phase2<K, PCK>(c, lb, cc.rbase, f, tile + row * TW + 4 * u4, H * TW, J.out_big != 0, store);
+			else
 			{
-				const uint4 t = *reinterpret_cast<const uint4 *>(tile + (l * H + row) * TW + 4 * u4);
-				dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
+				u32 dg[4][PCK];
+#pragma unroll
+				for (int l = 0; l < PCK; ++l)
+				{
+					const uint4 t = *reinterpret_cast<const uint4 *>(tile + (l * H + row) * TW + 4 * u4);
+					dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
+				}
+				u32 res[4][K];
+				top = J.out_big ? carry_phase2_unrolled<K, PCK, true>(c, lb, cc.rbase, f, dg, res)
+				                : carry_phase2_unrolled<K, PCK, false>(c, lb, cc.rbase, f, dg, res);
+				if (store)
+				{
+#pragma unroll
+					for (int k = 0; k < K; ++k)
+						*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + 4 * u4) = make_uint4(res[0][k], res[1][k], res[2][k], res[3][k]);
+				}
 			}
-			u32 res[4][K];
-			const i32 top = J.out_big ? carry_phase2<K, PCK, true>(c, lb, cc.rbase, f, dg, res)
-			                          : carry_phase2<K, PCK, false>(c, lb, cc.rbase, f, dg, res);
 			const bool is_last = (row == H - 1) && (u4 == ng - 1) && (b == nb - 1);
 			if ((is_last || !store) && top >= (i32)(1u << lb)) decision = 1;
-			if (store)
-			{
-#pragma unroll
-				for (int k = 0; k < K; ++k)
-					*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + 4 * u4) = make_uint4(res[0][k], res[1][k], res[2][k], res[3][k]);
-			}
 		}
 		__syncthreads();
 
