@@ -17,6 +17,8 @@
 // the first LA levels (all H rows of 32 adjacent columns, all K primes, in
 // shared memory) and the row pass owns the last LB levels (one row of one
 // prime per CTA, 32 coefficients per thread in registers).
+#include <atomic>
+
 #include "kernels.h"
 
 namespace ab
@@ -881,18 +883,29 @@ size_t colpass_smem(const Geometry & g, int K)
 	return sizeof(u32) * ((size_t)K * g.H * TW + (size_t)g.H * (TW / 4) * K + 3 * (size_t)K * g.H);
 }
 
+// The dynamic shared-memory limit of a kernel is a per-device setting: set it
+// once for each device a process launches on (bit d of `done` = device d).
+template <typename Kernel>
+static cudaError_t allow_dynamic_smem(Kernel kernel, size_t smem, std::atomic<unsigned long long> & done)
+{
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess) return e;
+	const unsigned long long bit = 1ull << (dev & 63);
+	if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+	e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+	return e;
+}
+
 template <int LOG_R>
 static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	const u32 R = 1u << LOG_R;
 	const size_t smem = sizeof(u32) * (R + R / 16);
-	static bool attr = false;
-	if (!attr)
-	{
-		cudaError_t e = cudaFuncSetAttribute(k_rowpass<LOG_R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		if (e != cudaSuccess) return e;
-		attr = true;
-	}
+	static std::atomic<unsigned long long> attr_done{0};
+	const cudaError_t e = allow_dynamic_smem(k_rowpass<LOG_R>, smem, attr_done);
+	if (e != cudaSuccess) return e;
 	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
 	const dim3 grid((unsigned)(c.K * g.H), (unsigned)njobs, (unsigned)ncand);
 	k_rowpass<LOG_R><<<grid, RowCfg<LOG_R>::NT, smem, s>>>(jobs, c);
@@ -921,13 +934,9 @@ template <int LOG_H, int K, int PCK>
 static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
 	const size_t smem = colpass_smem(g, K);
-	static bool attr = false;
-	if (!attr)
-	{
-		cudaError_t e = cudaFuncSetAttribute(k_colpass<LOG_H, K, PCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		if (e != cudaSuccess) return e;
-		attr = true;
-	}
+	static std::atomic<unsigned long long> attr_done{0};
+	const cudaError_t e = allow_dynamic_smem(k_colpass<LOG_H, K, PCK>, smem, attr_done);
+	if (e != cudaSuccess) return e;
 	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
 	const dim3 grid(g.R / CC, (unsigned)njobs, (unsigned)ncand);
 	k_colpass<LOG_H, K, PCK><<<grid, COL_THREADS, smem, s>>>(jobs, c);

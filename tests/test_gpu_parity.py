@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 # (K, ln, lbase) -- pck follows from K (1, 2, 2, 4)
 KERNEL_CASES = [
     (5, 6, 18), (5, 8, 18), (5, 10, 18), (5, 12, 18), (5, 13, 17), (5, 15, 17),
-    (4, 11, 28), (4, 16, 27), (3, 9, 22), (2, 10, 14), (5, 19, 17),
+    (4, 11, 28), (4, 16, 27), (3, 9, 22), (2, 10, 14), (5, 19, 17), (5, 20, 16),
 ]
 
 
