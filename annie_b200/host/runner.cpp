@@ -94,6 +94,7 @@ struct Class
 	std::vector<uint8_t> snap;
 	std::vector<int> count;
 	bool tuned = false;
+	size_t bytes = 0;                  // device memory of the batch
 };
 
 std::string hex64(uint64_t u)
@@ -162,6 +163,24 @@ struct ab_runner
 		return true;
 	}
 
+	// frees the batches that hold no test, so that tests of other size classes
+	// can be admitted once the budget is spent (a long-running server sees
+	// many sizes over time)
+	void reclaim()
+	{
+		for (auto it = classes.begin(); it != classes.end();)
+		{
+			Class & c = **it;
+			if (std::all_of(c.slots.begin(), c.slots.end(), [](Job * j) { return j == nullptr; }))
+			{
+				ab_batch_destroy(c.b);
+				used -= c.bytes;
+				it = classes.erase(it);
+			}
+			else ++it;
+		}
+	}
+
 	Class * class_for(const ab_params & p, bool create)
 	{
 		for (auto & c : classes)
@@ -170,6 +189,7 @@ struct ab_runner
 		if (!create) return nullptr;
 		ab_params cls = p; cls.lbase = 0;
 		const size_t per = ab_batch_slot_bytes(&cls);
+		if (used + per > o.hbm_budget_bytes) reclaim();
 		if (used + per > o.hbm_budget_bytes) return nullptr;
 		const int cap = (int)std::min<size_t>((size_t)o.max_slots_per_class, (o.hbm_budget_bytes - used) / per);
 		if (cap < 1) return nullptr;
@@ -179,7 +199,8 @@ struct ab_runner
 		c->slots.assign(cap, nullptr);
 		c->mult.assign((size_t)o.chunk * cap, 0);
 		c->snap.assign((size_t)o.chunk * cap, 0);
-		used += per * cap;
+		c->bytes = per * cap;
+		used += c->bytes;
 		classes.push_back(std::move(c));
 		return classes.back().get();
 	}

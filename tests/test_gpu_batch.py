@@ -192,3 +192,24 @@ def test_load_many_equals_single_loads():
             t.square_mul(int(mult[i, s]))
         assert np.array_equal(b.slot(s).read_register(0), t.read_register(0)), "slot %d" % s
         assert b.slot(s).get(0) == pow(int(mult[0, s]), 255, N)       # 8 steps of r = m r^2 from r = 1
+
+
+def test_runner_frees_idle_batches_for_other_sizes():
+    # a budget that holds one batch of one slot: the second size class can only
+    # be admitted once the first test is done and its idle batch freed
+    small = random_N(20000, 1)
+    big = random_N(60000, 2)
+    pb, _ = A.probe(big, 3)
+    ps, _ = A.probe(small, 3)
+    assert pb[:3] != ps[:3]
+    budget = max(A.lib().ab_batch_slot_bytes(A.Params(*pb[:3], 0)), A.lib().ab_batch_slot_bytes(A.Params(*ps[:3], 0)))
+    r = A.Runner(chunk=32, max_slots_per_class=4, hbm_budget_bytes=budget)
+    r.submit(small, base=3, tag=1)
+    r.submit(big, base=3, tag=2)
+    a, q = r.advance()
+    assert a == 1 and q == 1
+    res = _run_all(r)
+    assert set(res) == {1, 2}
+    for tag, N in ((1, small), (2, big)):
+        solo = A.prp_check(N, base=3)
+        assert res[tag]["status"] == 0 and res[tag]["res64"] == solo["res64"]
