@@ -94,6 +94,7 @@ ABI = [
     ("ab_square_mul_bits", [C.c_void_p, _u64p, C.c_size_t, C.c_int32], C.c_int),
     ("ab_set_geometry", [C.c_void_p, C.c_int], C.c_int),
     ("ab_get_geometry", [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    ("ab_set_overlap", [C.c_void_p, C.c_int], C.c_int),
     ("ab_timer_start", [C.c_void_p], C.c_int),
     ("ab_timer_stop", [C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     ("ab_last_error", [], C.c_char_p),
@@ -259,6 +260,10 @@ class Transform:
         rl, cl = C.c_int(), C.c_int()
         _check(self.L.ab_get_geometry(self.h, C.byref(rl), C.byref(cl)))
         return rl.value, cl.value
+
+    def set_overlap(self, on):
+        """Q-domain chain on a second stream (True, default) or one stream for everything."""
+        _check(self.L.ab_set_overlap(self.h, int(bool(on))))
 
     def mul(self, dst, src):
         _check(self.L.ab_mul(self.h, dst, src))

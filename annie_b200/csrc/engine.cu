@@ -160,6 +160,42 @@ bool compute_R_Ninv(const mpz_t N, const ab_params & p, mpz_t R, mpz_t Ninv, mpz
 }
 } // namespace
 
+// ============================================================ allocation-free squaring
+// Work buffers of ab_square_mul_noalloc: five registers of at most
+// AB_NOALLOC_MAX_WORDS words each (10 MiB), in a static device array that
+// every GPU loading this library holds until the process exits.  Host code
+// cannot use the symbol as an address: the device address is fetched with
+// cudaGetSymbolAddress, with that device current, once per device -- when a
+// transform or a batch is created there, so that the entry point itself only
+// queues kernels.
+#define AB_NOALLOC_MAX_WORDS (1u << 19)
+#define AB_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) u32 g_noalloc_scratch[5 * AB_NOALLOC_MAX_WORDS];
+
+namespace
+{
+std::mutex g_noalloc_mu;
+u32 * g_noalloc_addr[AB_NOALLOC_MAX_DEVICES] = {};
+
+u32 * noalloc_scratch(int device)
+{
+	if (device < 0 || device >= AB_NOALLOC_MAX_DEVICES) throw ab_error(AB_E_ARG, "device index out of range");
+	std::lock_guard<std::mutex> lock(g_noalloc_mu);
+	if (g_noalloc_addr[device] == nullptr)
+	{
+		int prev = 0;
+		CK(cudaGetDevice(&prev));
+		CK(cudaSetDevice(device));
+		void * p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		cudaSetDevice(prev);
+		if (e != cudaSuccess) throw ab_error(AB_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+		g_noalloc_addr[device] = static_cast<u32 *>(p);
+	}
+	return g_noalloc_addr[device];
+}
+}
+
 // ============================================================ the engine
 struct ab_transform
 {
@@ -186,6 +222,7 @@ struct ab_transform
 	void * flush_buf = nullptr;
 
 	u32 * bufp[NBUF] = {};   // device buffers (a batch slot view points into its batch)
+	u32 * noalloc = nullptr; // device address of the static scratch of ab_square_mul_noalloc on this device
 	bool view = false;       // true: memory and streams belong to a batch
 
 	// runs of squarings replayed from a captured CUDA graph: GRAPH_STEPS
@@ -582,6 +619,7 @@ struct ab_transform
 		if (failed) return;
 
 		CK(cudaSetDevice(device));
+		noalloc = noalloc_scratch(device);
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 		CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
 		CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
@@ -697,40 +735,6 @@ struct ab_batch
 	}
 };
 
-// ============================================================ allocation-free squaring
-// Work buffers of ab_square_mul_noalloc: five registers of at most
-// AB_NOALLOC_MAX_WORDS words each (10 MiB), in a static device array that
-// every GPU loading this library holds until the process exits.  Host code
-// cannot use the symbol as an address: the device address is fetched once
-// per device with cudaGetSymbolAddress, with that device current.
-#define AB_NOALLOC_MAX_WORDS (1u << 19)
-#define AB_NOALLOC_MAX_DEVICES 64
-static __device__ __align__(256) u32 g_noalloc_scratch[5 * AB_NOALLOC_MAX_WORDS];
-
-namespace
-{
-std::mutex g_noalloc_mu;
-u32 * g_noalloc_addr[AB_NOALLOC_MAX_DEVICES] = {};
-
-u32 * noalloc_scratch(int device)
-{
-	if (device < 0 || device >= AB_NOALLOC_MAX_DEVICES) throw ab_error(AB_E_ARG, "device index out of range");
-	std::lock_guard<std::mutex> lock(g_noalloc_mu);
-	if (g_noalloc_addr[device] == nullptr)
-	{
-		int prev = 0;
-		CK(cudaGetDevice(&prev));
-		CK(cudaSetDevice(device));
-		void * p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-		cudaSetDevice(prev);
-		if (e != cudaSuccess) throw ab_error(AB_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-		g_noalloc_addr[device] = static_cast<u32 *>(p);
-	}
-	return g_noalloc_addr[device];
-}
-}
-
 // ============================================================ C ABI
 namespace
 {
@@ -819,7 +823,11 @@ int ab_copy(ab_transform * h, size_t dst, size_t src)
 
 int ab_square_mul(ab_transform * h, int32_t a)
 {
-	return guarded([&] { need_ready(h); h->square_mul((u32)a); });
+	return guarded([&] {
+		need_ready(h);
+		if (a < 1) throw ab_error(AB_E_ARG, "multiplier a must be >= 1");
+		h->square_mul((u32)a);
+	});
 }
 
 int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, int32_t a)
@@ -849,6 +857,18 @@ int ab_set_geometry(ab_transform * h, int row_levels)
 		need_ready(h);
 		if (h->view) throw ab_error(AB_E_ARG, "a batch slot takes the geometry of its batch");
 		h->set_geometry(row_levels);
+	});
+}
+
+int ab_set_overlap(ab_transform * h, int on)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (h->view) throw ab_error(AB_E_ARG, "a batch slot runs on its batch's stream");
+		CK(cudaStreamSynchronize(h->st));
+		CK(cudaStreamSynchronize(h->st2));
+		h->overlap = (on != 0);
+		if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }   // captured with the old schedule
 	});
 }
 
@@ -1024,12 +1044,12 @@ int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg, int32_t a)
 {
 	return guarded([&] {
 		need_ready(h);
-		if (reg == nullptr) throw ab_error(AB_E_ARG, "null register");
+		if (reg == nullptr || a < 1) throw ab_error(AB_E_ARG, "null register or multiplier a < 1");
 		const size_t words = (size_t)h->prm.K * h->n;
 		if (words > AB_NOALLOC_MAX_WORDS)
 			throw ab_error(AB_E_CAPACITY, "ab_square_mul_noalloc: K*n = " + std::to_string(words) +
 				" words exceeds the static scratch limit of " + std::to_string(AB_NOALLOC_MAX_WORDS) + " words per register");
-		u32 * const s = noalloc_scratch(h->device);
+		u32 * const s = (h->noalloc != nullptr) ? h->noalloc : noalloc_scratch(h->device);
 		u32 * const aq0 = s, * const ar0 = s + AB_NOALLOC_MAX_WORDS, * const aq1 = s + 2 * AB_NOALLOC_MAX_WORDS;
 		u32 * const ar1 = s + 3 * AB_NOALLOC_MAX_WORDS, * const tq = s + 4 * AB_NOALLOC_MAX_WORDS;
 		using T = ab_transform;
@@ -1191,6 +1211,7 @@ void batch_install(ab_batch * b, int slot, std::unique_ptr<ab_transform> & vp, c
 	delete b->views[slot];
 	b->views[slot] = nullptr;
 	v->device = b->device; v->st = b->st; v->overlap = false;
+	v->noalloc = noalloc_scratch(b->device);
 	v->use_geometry(b->geo);             // the batch's split, which the autotuner may have changed
 	for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
 	v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
@@ -1255,6 +1276,7 @@ int ab_batch_clone(ab_batch * b, int dst, int src)
 		mpz_set(v->N, s->N); mpz_set(v->factor, s->factor);
 		v->prm = s->prm; v->n = s->n; v->geo = s->geo; v->tc = s->tc; v->failed = s->failed;
 		v->device = b->device; v->st = b->st; v->overlap = false;
+		v->noalloc = s->noalloc;
 		v->host.assign(b->words, 0);
 		for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)dst * b->words;
 		v->bufp[ab_transform::WR] = b->base[ab_transform::WR];

@@ -95,6 +95,7 @@ struct Class
 	std::vector<int> count;
 	bool tuned = false;
 	size_t bytes = 0;                  // device memory of the batch
+	uint64_t last_used = 0;            // runner tick of the last chunk or admission
 };
 
 std::string hex64(uint64_t u)
@@ -113,6 +114,7 @@ struct ab_runner
 	std::vector<std::unique_ptr<Class>> classes;
 	size_t used = 0;
 	uint64_t squarings = 0;
+	uint64_t tick = 0;                 // advance() calls
 
 	~ab_runner()
 	{
@@ -163,21 +165,25 @@ struct ab_runner
 		return true;
 	}
 
-	// frees the batches that hold no test, so that tests of other size classes
-	// can be admitted once the budget is spent (a long-running server sees
-	// many sizes over time)
-	void reclaim()
+	// frees batches that hold no test, least recently used first, until `need`
+	// more bytes fit the budget, so that tests of other size classes can be
+	// admitted once the budget is spent (a long-running server sees many sizes
+	// over time); the batches that stay keep their graphs and tuned split
+	void reclaim(size_t need)
 	{
-		for (auto it = classes.begin(); it != classes.end();)
+		while (used + need > o.hbm_budget_bytes)
 		{
-			Class & c = **it;
-			if (std::all_of(c.slots.begin(), c.slots.end(), [](Job * j) { return j == nullptr; }))
+			auto victim = classes.end();
+			for (auto it = classes.begin(); it != classes.end(); ++it)
 			{
-				ab_batch_destroy(c.b);
-				used -= c.bytes;
-				it = classes.erase(it);
+				const Class & c = **it;
+				if (!std::all_of(c.slots.begin(), c.slots.end(), [](Job * j) { return j == nullptr; })) continue;
+				if (victim == classes.end() || c.last_used < (*victim)->last_used) victim = it;
 			}
-			else ++it;
+			if (victim == classes.end()) return;
+			ab_batch_destroy((*victim)->b);
+			used -= (*victim)->bytes;
+			classes.erase(victim);
 		}
 	}
 
@@ -185,11 +191,11 @@ struct ab_runner
 	{
 		for (auto & c : classes)
 			if (c->cls.K == p.K && c->cls.pck == p.pck && c->cls.ln == p.ln)
-				for (Job * s : c->slots) if (s == nullptr) return c.get();
+				for (Job * s : c->slots) if (s == nullptr) { c->last_used = tick; return c.get(); }
 		if (!create) return nullptr;
 		ab_params cls = p; cls.lbase = 0;
 		const size_t per = ab_batch_slot_bytes(&cls);
-		if (used + per > o.hbm_budget_bytes) reclaim();
+		if (used + per > o.hbm_budget_bytes) reclaim(per);
 		if (used + per > o.hbm_budget_bytes) return nullptr;
 		const int cap = (int)std::min<size_t>((size_t)o.max_slots_per_class, (o.hbm_budget_bytes - used) / per);
 		if (cap < 1) return nullptr;
@@ -200,6 +206,7 @@ struct ab_runner
 		c->mult.assign((size_t)o.chunk * cap, 0);
 		c->snap.assign((size_t)o.chunk * cap, 0);
 		c->bytes = per * cap;
+		c->last_used = tick;
 		used += c->bytes;
 		classes.push_back(std::move(c));
 		return classes.back().get();
@@ -372,6 +379,7 @@ struct ab_runner
 			if (n > 0) any = true;
 		}
 		if (!any) return false;
+		c.last_used = tick;
 		ck(ab_batch_steps(c.b, S, c.mult.data(), c.snap.data()));
 		return true;
 	}
@@ -438,6 +446,7 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 	if (r == nullptr) return AB_E_ARG;
 	try
 	{
+		++r->tick;
 		r->admit();
 		std::vector<Class *> ran;
 		for (auto & c : r->classes) if (r->launch_class(*c)) ran.push_back(c.get());

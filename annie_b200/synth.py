@@ -68,3 +68,54 @@ def random_odd(bits, seed):
 
 def proth(k, n):
     return k * (1 << n) + 1
+
+
+def jacobi(a, n):
+    """Jacobi symbol (a/n), n odd positive."""
+    a %= n
+    r = 1
+    while a:
+        while a % 2 == 0:
+            a //= 2
+            if n % 8 in (3, 5):
+                r = -r
+        a, n = n, a
+        if a % 4 == 3 and n % 4 == 3:
+            r = -r
+        a %= n
+    return r if n == 1 else 0
+
+
+def euler_base(N):
+    """Smallest non-square a >= 2 with (a/N) = -1: the Euler-test base rule of the
+    reference driver (src/annie.h:250-253)."""
+    import math
+    a = 2
+    while jacobi(a, N) != -1:
+        a += 1
+        s = math.isqrt(a)
+        if s * s == a:
+            a += 1
+    return a
+
+
+# The workloads the benchmarks and the parity tests share.
+FERMAT_33M_BITS, FERMAT_33M_SEED = 33219281, 2
+
+
+def fermat_33m():
+    """The 33,219,281-bit random odd N (about 10 M digits) tested with base 3."""
+    return random_odd(FERMAT_33M_BITS, FERMAT_33M_SEED)
+
+
+def proth_2m(n=2000000, seed=11, usable=None):
+    """Proth number k*2^n + 1, k odd in [2^19, 2^20) drawn from seed `seed`, and its
+    Euler base; `usable(N, a)` (optional) rejects draws, e.g. those whose N shares
+    a factor with the transform's R."""
+    rng = Xoshiro256ss(seed)
+    while True:
+        k = rng.uniform(1 << 19, 1 << 20) | 1
+        N = proth(k, n)
+        a = euler_base(N)
+        if usable is None or usable(N, a):
+            return k, N, a

@@ -24,6 +24,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -31,6 +33,7 @@ BITS = 33219281
 SEED = 2
 BASE = 3
 SQ_PER_STEP = 512
+PARITY_WINDOW = 8          # test-loop iterations compared word for word with the reference
 METRIC = "us_per_squaring_33.2Mbit"
 UNIT = "us/squaring"
 WORKLOAD = "Fermat PRP base 3, random odd 33,219,281-bit N (xoshiro256** seed 2), NTT 2^19 x 5 primes, 4x17-bit digits"
@@ -251,6 +254,19 @@ def run_ours(args, world, rank, local, pg):
         "kernels": kernels,
     }
 
+    # ---- parity window (the same window the CPU-baseline leg runs on the
+    # reference): Reg0 = 1, Reg1 = Reg0, PARITY_WINDOW iterations of the test
+    # loop from the top bit of E, then Reg1 *= Reg0; the registers are checked
+    # word for word after the run
+    t.set1()
+    t.copy(1, 0)
+    E = N - 1
+    for i in range(PARITY_WINDOW):
+        t.square_mul(BASE if (E >> (top - i)) & 1 else 1)
+    t.mul(1, 0)
+    regs = np.concatenate([t.read_register(0), t.read_register(1)])
+    t.close()
+
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 4),
@@ -266,20 +282,37 @@ def run_ours(args, world, rank, local, pg):
         "clocks": clk,
         "roofline": roof,
     }
-    return line
+    return line, regs
 
 
 def cpu_baseline_line(args, steps):
+    """The reference's transformCPU on the host cores over the first `steps`
+    iterations of the test loop (checker and CPU baseline: see oracle/cpu_baseline.py)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cpu_baseline
     res = cpu_baseline.run(BITS, SEED, BASE, squarings=steps)
     return res
 
 
+def parity_record(gpu_regs, res):
+    """Word-for-word comparison of Reg0 || Reg1 after the parity window."""
+    ref = res.get("regs") if res else None
+    if ref is None:
+        return {"checked": False, "equal": None, "why": "the reference's transformCPU is not built here"}
+    ref = np.asarray(ref, dtype=np.uint32)
+    n = min(len(ref), len(gpu_regs))
+    diff = int(np.count_nonzero(ref[:n] != gpu_regs[:n])) + abs(len(ref) - len(gpu_regs))
+    return {"checked": True, "equal": diff == 0, "words": int(len(gpu_regs)), "words_differing": diff,
+            "against": "reference transformCPU (src/transformCPU.h), compiled from the reference sources",
+            "window": "Reg0 = 1, Reg1 = Reg0, %d test-loop iterations from the top bit of E = N - 1, "
+                      "then Reg1 *= Reg0; raw register words of Reg0 and Reg1" % PARITY_WINDOW}
+
+
 def run_reference(args, world, rank, pg):
     if rank != 0:
         return None
-    res = cpu_baseline_line(args, max(1, min(16, args.steps // 5)))     # about 15 s of CPU per process
+    per_proc = max(1, min(16, args.steps // 5))            # about 15 s of CPU per process
+    res = cpu_baseline_line(args, per_proc)
     v = res["value_us"]
     return {
         "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -287,10 +320,16 @@ def run_reference(args, world, rank, pg):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded random N)",
         "impl": "reference",
         "config": {"workload": WORKLOAD, "squarings_per_step": SQ_PER_STEP},
+        "extrapolated": True,
+        "timed_squarings": res["squarings"],
+        "timed_seconds": round(res["seconds"], 3),
+        "note": "value = the squarings actually timed (%d processes x %d, the first test-loop iterations) over the "
+                "slowest process's time; ms_per_step extrapolates that rate to %d squarings per step"
+                % (res["cores"], per_proc, SQ_PER_STEP),
         "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": res["cores"], "kind": "reference",
                          "sample": "reference transformCPU (src/transformCPU.h) compiled from the reference sources, "
                                    "%d processes x %d squarings at 33.2M bits, set-up untimed; one core: %.0f us/squaring"
-                                   % (res["cores"], res["squarings"] // res["cores"], res["single_us"])},
+                                   % (res["cores"], per_proc, res["single_us"])},
         "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -551,14 +590,8 @@ def run_proth2m_workload(args):
     B iterations included), then one Gerbicz-Li check and an injected single-word
     error that the next check detects and rolls back."""
     import annie_b200 as A
-    from annie_b200.synth import Xoshiro256ss, proth
-    rng = Xoshiro256ss(11)
-    while True:
-        k = rng.uniform(1 << 19, 1 << 20) | 1
-        N = proth(k, args.proth_n)
-        a = _euler_base(N)
-        if not A.probe(N, a)[1]:
-            break
+    from annie_b200.synth import proth_2m
+    k, N, a = proth_2m(args.proth_n, 11, usable=lambda N, a: not A.probe(N, a)[1])
     t = A.Transform(N, a)
     E = (N - 1) >> 1
     B = _gl_block(E.bit_length())
@@ -689,17 +722,34 @@ def main():
         if line is not None:
             print(json.dumps(line), flush=True)
         return
-    line = run_ours(args, world, rank, local, pg)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res = cpu_baseline_line(args, 2)
-        line["cpu_baseline"] = {
-            "value": round(res["value_us"], 3), "unit": UNIT, "cores": res["cores"], "kind": "reference",
-            "sample": "reference transformCPU compiled from its sources, %d processes x 2 squarings at 33.2M bits "
-                      "(set-up untimed); one core: %.0f us/squaring" % (res["cores"], res["single_us"])}
+    line, regs = run_ours(args, world, rank, local, pg)
     if pg is not None:
         pg.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    if rank != 0:
+        return
+    res = None
+    if not args.no_cpu_baseline:
+        try:
+            # rank 0: the reference over the parity window (at N > 1 one process,
+            # only to check this rank's registers)
+            procs = None if world == 1 else 1
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import cpu_baseline
+            res = cpu_baseline.run(BITS, SEED, BASE, squarings=PARITY_WINDOW, procs=procs)
+        except RuntimeError as e:
+            res = None
+            sys.stderr.write("no reference run: %s\n" % e)
+    if res is not None and world == 1:
+        line["cpu_baseline"] = {
+            "value": round(res["value_us"], 3), "unit": UNIT, "cores": res["cores"], "kind": "reference",
+            "sample": "reference transformCPU compiled from its sources, %d processes x %d squarings (the first test-loop "
+                      "iterations) at 33.2M bits, set-up untimed; one core: %.0f us/squaring"
+                      % (res["cores"], PARITY_WINDOW, res["single_us"])}
+    line["parity"] = parity_record(regs, res)
+    print(json.dumps(line), flush=True)
+    if line["parity"]["checked"] and not line["parity"]["equal"]:
+        sys.stderr.write("PARITY FAILURE: registers differ from the reference after the window\n")
+        sys.exit(3)
 
 
 if __name__ == "__main__":

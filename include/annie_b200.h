@@ -61,7 +61,7 @@ int ab_info(const ab_transform * h, ab_params * out);                /* transfor
 
 int ab_set1(ab_transform * h);                                       /* transform::set1  (transform.h:26, transformGPU.h:571-574) */
 int ab_copy(ab_transform * h, size_t dst, size_t src);               /* transform::copy  (transform.h:28, transformGPU.h:588-591) */
-int ab_square_mul(ab_transform * h, int32_t a);                      /* transform::square_mul (transform.h:29, transformGPU.h:593-596) */
+int ab_square_mul(ab_transform * h, int32_t a);                      /* transform::square_mul (transform.h:29, transformGPU.h:593-596); a >= 1 */
 int ab_mul(ab_transform * h, size_t dst, size_t src);                /* transform::mul   (transform.h:30, transformGPU.h:598-601) */
 /* transform::get (transform.h:27, transformGPU.h:576-586): r_src out of
    MMGW form, reduced mod N; `count` = limbs written. */
@@ -102,6 +102,11 @@ int ab_square_mul_bits(ab_transform * h, const uint64_t * bits, size_t count, in
 int ab_set_geometry(ab_transform * h, int row_levels);
 int ab_get_geometry(const ab_transform * h, int * row_levels, int * col_levels);
 
+/* Schedule of a squaring: on != 0 (default) runs the Q-domain chain on a
+   second stream beside the R-domain chain; on = 0 runs every launch on the
+   handle's stream.  The registers do not depend on it (determinism tests). */
+int ab_set_overlap(ab_transform * h, int on);
+
 /* Device time of the work queued since the last call, in milliseconds
    (CUDA events on the handle's stream). */
 int ab_timer_start(ab_transform * h);
@@ -135,10 +140,11 @@ int ab_flush_l2(ab_transform * h, size_t bytes);
  * ab_square_mul does for Reg0.  The work buffers come from a static device
  * array of 5 x 2^19 words (10 MiB) that every GPU loading this library holds
  * until exit, so K*n must not exceed 2^19 words (else AB_E_CAPACITY).  No
- * cudaMalloc, cudaFree or allocating library call is made.  The first call on
- * a device looks up the array's device address (cudaGetSymbolAddress, with
- * that device current); make that first call before any stream capture.
- * Work is queued on the handle's stream (ab_synchronize waits for it).  All
+ * cudaMalloc, cudaFree or allocating library call is made: the array's device
+ * address is looked up (cudaGetSymbolAddress, with the device current) when
+ * the handle is created, so a call only queues kernels.  a must be >= 1
+ * (else AB_E_ARG).  Work is queued on the handle's stream (ab_synchronize
+ * waits for it).  All
  * calls share the one array: calls whose work overlaps on the GPU (other
  * handles' streams, other host threads) race and give wrong results. */
 int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg_device, int32_t a);

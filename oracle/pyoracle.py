@@ -19,9 +19,14 @@ _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
 
 
-def build(ref_src="/root/reference/src"):
-    """Build _ref/liboracle.so (and _ref/libannie_ref.so when the reference sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE, "REF_SRC=" + ref_src], check=True)
+def build(ref_src=None):
+    """Build _ref/liboracle.so, and _ref/libannie_ref.so when the reference's src
+    folder is given (argument, or the ANNIE_REF_SRC environment variable)."""
+    ref_src = ref_src or os.environ.get("ANNIE_REF_SRC", "")
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_src:
+        cmd.append("REF_SRC=" + ref_src)
+    subprocess.run(cmd, check=True)
 
 
 def int_to_limbs(x):
