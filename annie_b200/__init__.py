@@ -90,6 +90,7 @@ ABI = [
     ("ab_host_free", [C.c_void_p], None),
     ("ab_read_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
     ("ab_write_register", [C.c_void_p, C.c_size_t, _u32p, C.c_size_t], C.c_int),
+    ("ab_inject_word", [C.c_void_p, C.c_size_t, C.c_size_t, C.c_int32], C.c_int),
     ("ab_synchronize", [C.c_void_p], C.c_int),
     ("ab_square_mul_bits", [C.c_void_p, _u64p, C.c_size_t, C.c_int32], C.c_int),
     ("ab_set_geometry", [C.c_void_p, C.c_int], C.c_int),
@@ -318,6 +319,10 @@ class Transform:
         w = np.ascontiguousarray(words, dtype=np.uint32)
         _check(self.L.ab_write_register(self.h, reg, w.ctypes.data_as(_u32p), len(w)))
 
+    def inject_word(self, reg, index, delta=-1):
+        """Adds delta to one 32-bit word of the engine's copy of register reg (fault injection)."""
+        _check(self.L.ab_inject_word(self.h, reg, index, delta))
+
     def synchronize(self):
         _check(self.L.ab_synchronize(self.h))
 
@@ -349,22 +354,24 @@ class Transform:
 
     # -- information strings (transformGPU.h:766-795)
     def get_info_short(self):
-        return "%d-prime NTT of length %d, packed-base = 2^{%dx%d}" % (self.K, self.n, self.pck, self.lbase)
+        return "%d-prime NTT of length %d, packed-base = 2^{%dx%d}" % (self.K + 1, self.n, self.pck, self.lbase)
 
     def get_info(self):
         return "Montgomery-McLaughlin-Gallot-Woltman reduction, " + self.get_info_short()
 
     # -- diagnostics
     def diag_forward(self, words, domain_q):
+        """Forward NTT of a normal-form register over the engine's K+1 transform primes."""
         w = np.ascontiguousarray(words, dtype=np.uint32)
-        out = np.zeros_like(w)
+        out = np.zeros((self.K + 1) * self.n, dtype=np.uint32)
         _check(self.L.ab_diag_forward(self.h, int(domain_q), w.ctypes.data_as(_u32p), out.ctypes.data_as(_u32p)))
         return out
 
-    def diag_product(self, words, domain_q, a, xp=None, sub=None, lower_mode=0):
+    def diag_product(self, words, domain_q, a, y=None, sub=None, lower_mode=0):
+        """Product (square when y is None) of normal-form registers in one domain, then the carry."""
         w = np.ascontiguousarray(words, dtype=np.uint32)
         out = np.zeros_like(w)
-        xpa = None if xp is None else np.ascontiguousarray(xp, dtype=np.uint32)
+        xpa = None if y is None else np.ascontiguousarray(y, dtype=np.uint32)
         sba = None if sub is None else np.ascontiguousarray(sub, dtype=np.uint32)
         _check(self.L.ab_diag_product(self.h, int(domain_q), w.ctypes.data_as(_u32p),
                                       None if xpa is None else xpa.ctypes.data_as(_u32p), a,

@@ -42,14 +42,24 @@ struct ab_error : std::runtime_error
 
 // ------------------------------------------------------------ host Z/pZ
 // The 14 primes of the reference and their primitive roots
-// (src/transformGPU.h:79-89).
+// (src/transformGPU.h:79-89): the parameter rule and the register words of
+// the reference's normal form use them.
 const u32 PRIMES[14] = {
 	(125u << 25) + 1, (243u << 24) + 1, (235u << 24) + 1, (29u << 27) + 1,
 	(13u << 28) + 1, (193u << 24) + 1, (3u << 30) + 1, (43u << 26) + 1,
 	(171u << 24) + 1, (81u << 25) + 1, (157u << 24) + 1, (151u << 24) + 1,
 	(37u << 26) + 1, (17u << 27) + 1 };
-const u32 PRIMROOTS[14] = { 3, 7, 3, 3, 3, 3, 5, 3, 35, 5, 3, 3, 3, 3 };
 
+// The transform primes: p < 2^30, p = c 2^23 + 1 (roots of unity of order
+// 2^23 cover both domains up to n = 2^22), largest first, with a generator of
+// each multiplicative group.  A class with K reference primes uses the first
+// K + 1: their product exceeds the reference's (2^89.4 > 2^63.9 for K = 2,
+// 2^118.8 > 2^95.8, 2^148.1 > 2^127.6, 2^177.3 > 2^159.3 for K = 5).
+const u32 TPRIMES[AB_MAXKP] = { 119u * (1u << 23) + 1, 107u * (1u << 23) + 1, 105u * (1u << 23) + 1,
+                                90u * (1u << 23) + 1, 77u * (1u << 23) + 1, 71u * (1u << 23) + 1 };
+const u32 TGEN[AB_MAXKP] = { 3, 3, 26, 11, 3, 3 };
+
+// Montgomery arithmetic mod a reference prime (canonical values)
 struct HostZp
 {
 	u32 p, q, one, rsq;
@@ -59,7 +69,6 @@ struct HostZp
 		one = (u32)(((u64)1 << 32) % p);
 		rsq = (u32)(((u64)one * one) % p);
 	}
-	u32 add(u32 a, u32 b) const { return a + b - ((a >= p - b) ? p : 0); }
 	u32 sub(u32 a, u32 b) const { return a - b + ((a < b) ? p : 0); }
 	u32 mul(u32 a, u32 b) const
 	{
@@ -71,6 +80,17 @@ struct HostZp
 	u32 inv(u32 x) const { return pow(x, p - 2); }
 };
 
+// Plain arithmetic mod a transform prime
+struct TZp
+{
+	u32 p;
+	explicit TZp(u32 pp) : p(pp) {}
+	u32 mul(u32 a, u32 b) const { return (u32)(((u64)a * b) % p); }
+	u32 pow(u32 x, u64 e) const { u32 r = 1; while (e) { if (e & 1) r = mul(r, x); x = mul(x, x); e >>= 1; } return r; }
+	u32 inv(u32 x) const { return pow(x, p - 2); }
+	u32 shoup(u32 w) const { return (u32)(((u64)w << 32) / p); }
+};
+
 size_t bitrev(size_t i, size_t n)
 {
 	size_t r = 0;
@@ -78,38 +98,34 @@ size_t bitrev(size_t i, size_t n)
 	return r;
 }
 
-// Twiddles w[S + bitrev(j, S)], S = n/4 .. 1, inverse at +n/2; w[0] is the
-// Montgomery form of w[1].  Domain R (x^n - 1) uses roots of unity of order
-// 2S, domain Q (x^n + 1) the twisted roots of order 4S (transformGPU.h:117-160).
-void make_roots(u32 * w, int ln, int k, bool domain_q)
+// Twiddle tables of transform prime k for length 2^ln, as Shoup pairs
+// (w, floor(w 2^32 / p)) at the reference's positions s + bitrev(j, s),
+// s = n/4 .. 1 (transformGPU.h:117-160; position 0 unused).  Domain R
+// (x^n - 1): w = rho_s^j with rho_s a primitive 2s-th root of unity, and
+// wi = -rho_s^-j.  Domain Q (x^n + 1), twisted: w = psi_s rho_s^j with psi_s a
+// primitive 4s-th root (psi_s^2 = rho_s); it needs no inverse table, since
+// -w_j^-1 = w_{s-1-j}, which sits at the mirrored position.
+void make_twiddles(uint2 * w, uint2 * wi, int ln, int k, bool domain_q)
 {
-	const HostZp z(PRIMES[k]);
+	const TZp z(TPRIMES[k]);
 	const size_t n = (size_t)1 << ln;
-	u32 * wi = w + n / 2;
-	auto primroot_n = [&](int l) { return z.pow(z.to_mont(PRIMROOTS[k]), (z.p - 1) >> l); };
-	if (!domain_q)
+	auto root = [&](int l) { return z.pow(TGEN[k], (z.p - 1) >> l); };     // primitive 2^l-th root
+	auto pair = [&](u32 v) { return make_uint2(v, z.shoup(v)); };
+	w[0] = make_uint2(0, 0);
+	if (wi) wi[0] = make_uint2(0, 0);
+	int l = ln - 1;                                  // rho of the level s = n/4 has order 2^(ln-1)
+	for (size_t s = n / 4; s >= 1; s /= 2, --l)
 	{
-		u32 sr = primroot_n(ln - 1), sri = z.inv(sr);
-		for (size_t s = n / 4; s >= 1; s /= 2)
+		const u32 rho = root(l), rhoi = z.inv(rho);
+		u32 t = domain_q ? root(l + 1) : 1u, ti = 1u;
+		for (size_t j = 0; j < s; ++j)
 		{
-			u32 t = z.one, ti = z.one;
-			for (size_t j = 0; j < s; ++j) { const size_t jr = bitrev(j, s); w[s + jr] = t; wi[s + jr] = ti; t = z.mul(t, sr); ti = z.mul(ti, sri); }
-			sr = z.mul(sr, sr); sri = z.mul(sri, sri);
+			const size_t jr = bitrev(j, s);
+			w[s + jr] = pair(t);
+			if (wi) wi[s + jr] = pair((z.p - ti) % z.p);
+			t = z.mul(t, rho); ti = z.mul(ti, rhoi);
 		}
 	}
-	else
-	{
-		u32 sr2 = primroot_n(ln), sr2i = z.inv(sr2);
-		for (size_t s = n / 4; s >= 1; s /= 2)
-		{
-			const u32 sr = z.mul(sr2, sr2), sri = z.mul(sr2i, sr2i);
-			u32 t = sr2, ti = sr2i;
-			for (size_t j = 0; j < s; ++j) { const size_t jr = bitrev(j, s); w[s + jr] = t; wi[s + jr] = ti; t = z.mul(t, sr); ti = z.mul(ti, sri); }
-			sr2 = sr; sr2i = sri;
-		}
-	}
-	w[0] = z.to_mont(w[1]);
-	wi[0] = 0;
 }
 
 size_t get_s(size_t K) { int s = -1; for (size_t k = K - 1; k != 0; k /= 2) ++s; return (size_t)1 << s; }
@@ -161,8 +177,9 @@ bool compute_R_Ninv(const mpz_t N, const ab_params & p, mpz_t R, mpz_t Ninv, mpz
 } // namespace
 
 // ============================================================ allocation-free squaring
-// Work buffers of ab_square_mul_noalloc: five registers of at most
-// AB_NOALLOC_MAX_WORDS words each (10 MiB), in a static device array that
+// Work buffers of ab_square_mul_noalloc: five regions of AB_NOALLOC_MAX_WORDS
+// words (10 MiB; four NTT-form buffers, then T_Q and the register's exact
+// values) and a flag word, in a static device array that
 // every GPU loading this library holds until the process exits.  Host code
 // cannot use the symbol as an address: the device address is fetched with
 // cudaGetSymbolAddress, with that device current, once per device -- when a
@@ -170,7 +187,7 @@ bool compute_R_Ninv(const mpz_t N, const ab_params & p, mpz_t R, mpz_t Ninv, mpz
 // queues kernels.
 #define AB_NOALLOC_MAX_WORDS (1u << 19)
 #define AB_NOALLOC_MAX_DEVICES 64
-static __device__ __align__(256) u32 g_noalloc_scratch[5 * AB_NOALLOC_MAX_WORDS];
+static __device__ __align__(256) u32 g_noalloc_scratch[5 * AB_NOALLOC_MAX_WORDS + 64];
 
 namespace
 {
@@ -199,7 +216,16 @@ u32 * noalloc_scratch(int device)
 // ============================================================ the engine
 struct ab_transform
 {
-	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, NQ, NIR, OPQ, OPR, AQ0, AQ1, AR0, AR1, TMP, SNAP, WR, WQ, NBUF };
+	// Device buffers.  Normal form (AB_NW = 3 planes of n words, exact
+	// coefficient values): the registers, the MMGW one, T_Q, TMP, the
+	// Gerbicz-Li snapshot.  NTT form (KP planes): the four partly transformed
+	// work buffers, the transforms of N (domain Q) and N^-1 (domain R), two
+	// transformed multiplicands.  Shared by the slots of a batch: XW (the
+	// reference's register words, K planes, for conversions) and the twiddle
+	// tables (KP n words each: n/2 Shoup pairs per prime).
+	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, TMP, SNAP, AQ0, AQ1, AR0, AR1, NQ, NIR, OPQ, OPR, NSLOT = OPR + 1,
+	           XW = NSLOT, WR, WRI, WQ, NBUF };
+	static bool normal_buf(int i) { return i <= SNAP; }
 
 	int device = 0;
 	cudaStream_t st = nullptr;
@@ -208,12 +234,15 @@ struct ab_transform
 	bool overlap = true;                 // run the Q chain on st2 (off for per-launch profiling)
 	bool split = false;                  // without overlap: still one launch per domain
 	ab_params prm{};
+	int KP = 0;                          // transform primes
 	size_t n = 0;
 	Geometry geo{};
 	TConst tc{};
+	RefConst rc{};
 	bool failed = false;
 	mpz_t N, factor;
 	u32 * dmem = nullptr;
+	u32 * d_flag = nullptr;              // import error flag (device word)
 	bool prefwd = false;     // AQ0/AR0 hold the first forward levels of REG0
 	std::vector<u32> host;
 	uint64_t launches = 0;   // kernels launched by this handle
@@ -237,6 +266,12 @@ struct ab_transform
 	int mult_i = 0;
 
 	u32 * b(int i) const { return bufp[i]; }
+	const uint2 * tw(int i) const { return reinterpret_cast<const uint2 *>(bufp[i]); }
+	size_t words_of(int i) const
+	{
+		if (i == XW) return (size_t)prm.K * n;
+		return (i < NSLOT && normal_buf(i)) ? (size_t)AB_NW * n : (size_t)KP * n;
+	}
 
 	ab_transform() { mpz_inits(N, factor, nullptr); }
 	ab_transform(const ab_transform &) = delete;
@@ -260,32 +295,65 @@ struct ab_transform
 		mpz_clears(N, factor, nullptr);
 	}
 
-	void build_consts()
+	// Constants of the transform primes (TConst) and of the reference primes
+	// (RefConst) for the class (K, pck, ln) and digit size lbase.
+	static void build_consts(const ab_params & prm, const Geometry & geo, TConst & tc, RefConst & rc)
 	{
-		const int K = prm.K;
+		const int K = prm.K, KP = K + 1, L = K;
+		const size_t n = (size_t)1 << prm.ln;
 		std::memset(&tc, 0, sizeof(tc));
-		tc.K = K; tc.pck = prm.pck; tc.lbase = prm.lbase; tc.ln = prm.ln;
+		tc.K = K; tc.KP = KP; tc.pck = prm.pck; tc.lbase = prm.lbase; tc.ln = prm.ln;
 		tc.n = (u32)n; tc.R = geo.R; tc.H = geo.H; tc.LA = geo.LA; tc.LB = geo.LB;
+		mpz_t M, Mk, t, mod; mpz_inits(M, Mk, t, mod, nullptr);
+		mpz_set_ui(M, 1);
+		for (int k = 0; k < KP; ++k) mpz_mul_ui(M, M, TPRIMES[k]);
+		mpz_set_ui(mod, 1); mpz_mul_2exp(mod, mod, (mp_bitcnt_t)32 * L);
+		auto limbs = [&](const mpz_t v, u32 * out) {
+			mpz_fdiv_r(t, v, mod);
+			for (int j = 0; j < L; ++j) { out[j] = (u32)mpz_get_ui(t); mpz_fdiv_q_2exp(t, t, 32); }
+		};
+		for (int k = 0; k < KP; ++k)
+		{
+			const TZp z(TPRIMES[k]);
+			const u32 p = z.p;
+			tc.p[k] = p;
+			u32 pinv = 1; for (int i = 0; i < 6; ++i) pinv *= 2 - p * pinv;
+			tc.pinv[k] = pinv;
+			tc.one_s[k] = z.shoup(1);
+			tc.c32[k] = (u32)(((u64)1 << 32) % p); tc.c32s[k] = z.shoup(tc.c32[k]);
+			tc.c64[k] = z.mul(tc.c32[k], tc.c32[k]); tc.c64s[k] = z.shoup(tc.c64[k]);
+			const u32 p95 = z.mul(tc.c64[k], (u32)(((u64)1 << 31) % p));
+			tc.k95[k] = (p - p95) % p;
+			mpz_divexact_ui(Mk, M, p);
+			const u32 mk_mod_p = (u32)mpz_fdiv_ui(Mk, p);
+			// (2/n) 2^32 (M/p)^-1: undoes the n/2 of the inverse levels and the
+			// 2^-32 of the Montgomery pointwise product, and weights the CRT
+			tc.crt[k] = z.mul(z.mul(z.inv((u32)((n / 2) % p)), tc.c32[k]), z.inv(mk_mod_p));
+			tc.crts[k] = z.shoup(tc.crt[k]);
+			tc.fl[k] = (u32)(((u64)1 << 60) / p);
+			limbs(Mk, tc.mk[k]);
+		}
+		mpz_neg(t, M);
+		limbs(t, tc.negm);
+		mpz_clears(M, Mk, t, mod, nullptr);
+
+		std::memset(&rc, 0, sizeof(rc));
+		rc.K = K;
 		for (int k = 0; k < K; ++k)
 		{
 			const HostZp z(PRIMES[k]);
-			tc.p[k] = z.p; tc.q[k] = z.q; tc.rsq[k] = z.rsq;
-			tc.norm[k] = z.p - ((z.p - 1) >> (prm.ln - 1));
-			const u32 base = (u32)((1ull << prm.lbase) % z.p);
-			tc.rbase[k] = z.to_mont(base);
-			u32 bp = 1; for (int l = 0; l < prm.pck; ++l) bp = (u32)(((u64)bp * base) % z.p);
-			tc.rbase_pck[k] = bp;
-			const u32 b2 = (u32)(((u64)base * base) % z.p);
-			tc.b2m[k] = z.to_mont(b2); tc.b2mq[k] = tc.b2m[k] * z.q;
+			rc.p[k] = z.p; rc.q[k] = z.q;
+			rc.r2[k] = (u32)((((u64)z.one) * z.one) % z.p);          // 2^64 mod p
 			for (int j = k + 1; j < K; ++j)
 			{
-				tc.gm[k][j] = z.inv(z.to_mont(PRIMES[j] % z.p));   // Montgomery form of P_j^-1
-				tc.gmq[k][j] = tc.gm[k][j] * z.q;
+				rc.gm[k][j] = z.inv(z.to_mont(PRIMES[j] % z.p));       // Montgomery form of P_j^-1
+				rc.gmq[k][j] = rc.gm[k][j] * z.q;
 			}
 		}
 	}
 
-	// integer -> RNS register words (transformGPU.h:323-360)
+	// integer -> exact coefficient values: pck digits of lbase bits per
+	// coefficient (transformGPU.h:323-360), three limb planes
 	void encode(const mpz_t x, u32 * out) const
 	{
 		const size_t nl = mpz_size(x);
@@ -304,41 +372,33 @@ struct ab_transform
 			u32 dg[4];
 			for (int l = 0; l < prm.pck; ++l) { dg[l] = read_bits(bit); bit += (size_t)lb; }
 			for (int l = prm.pck - 1; l >= 0; --l) d = (d << lb) | dg[l];
-			for (int k = 0; k < prm.K; ++k) out[(size_t)k * n + i] = (u32)(d % PRIMES[k]);
+			out[i] = (u32)d; out[n + i] = (u32)(d >> 32); out[2 * n + i] = (u32)(d >> 64);
 		}
 	}
 
-	// register words (first pck planes) -> integer y, then y mod N
-	// (transformGPU.h:362-445: CRT over the first pck primes, carry, pack)
+	// exact coefficient values -> integer sum_i v_i 2^(pck lbase i), then mod N
+	// (transformGPU.h:362-445 does the same from the residues)
 	void decode(const u32 * planes, mpz_t y) const
 	{
-		const int pck = prm.pck, lb = prm.lbase;
-		const size_t nbits = (size_t)pck * lb * n, nlimbs = nbits / 64 + 2;
+		const int w = prm.pck * prm.lbase;
+		const size_t nbits = (size_t)w * n, nlimbs = nbits / 64 + 2;
 		std::vector<u64> out(nlimbs, 0);
-		HostZp z[4] = { HostZp(PRIMES[0]), HostZp(PRIMES[1 % 14]), HostZp(PRIMES[2]), HostZp(PRIMES[3]) };
-		u32 inv[4][4] = {};
-		for (int i = 0; i < pck; ++i)
-			for (int j = i + 1; j < pck; ++j) inv[i][j] = z[i].mul(z[i].inv(z[i].to_mont(PRIMES[j] % z[i].p)), 1);
 		__int128 f = 0; size_t bit = 0;
+		auto put = [&](u64 r, int cnt) {
+			const size_t li = bit / 64; const int sh = (int)(bit % 64);
+			out[li] |= r << sh; if (sh != 0 && sh + cnt > 64) out[li + 1] |= r >> (64 - sh);
+			bit += (size_t)cnt;
+		};
 		for (size_t i = 0; i < n; ++i)
 		{
-			u32 u[4];
-			for (int ii = pck - 1; ii >= 0; --ii)
+			const unsigned __int128 u = (unsigned __int128)planes[i] | ((unsigned __int128)planes[n + i] << 32) |
+			                            ((unsigned __int128)planes[2 * n + i] << 64);
+			f += (__int128)(u << 32) >> 32;           // sign-extended 96-bit value
+			for (int left = w; left > 0;)
 			{
-				u32 v = planes[(size_t)ii * n + i];
-				for (int j = pck - 1; j > ii; --j) v = (u32)(((u64)z[ii].sub(v, u[j]) * inv[ii][j]) % z[ii].p);
-				u[ii] = v;
-			}
-			const int32_t i0 = (u[0] > z[0].p / 2) ? (int32_t)(u[0] - z[0].p) : (int32_t)u[0];
-			__int128 D = i0;
-			for (int ii = 1; ii < pck; ++ii) D = D * z[ii].p + u[ii];
-			f += D;
-			for (int l = 0; l < pck; ++l)
-			{
-				const u64 r = (u64)(f & (((__int128)1 << lb) - 1));
-				const size_t li = bit / 64; const int sh = (int)(bit % 64);
-				out[li] |= r << sh; if (sh != 0 && sh + lb > 64) out[li + 1] |= r >> (64 - sh);
-				f >>= lb; bit += (size_t)lb;
+				const int cnt = std::min(left, 32);
+				put((u64)(f & ((((__int128)1) << cnt) - 1)), cnt);
+				f >>= cnt; left -= cnt;
 			}
 		}
 		mpz_import(y, nlimbs, -1, 8, 0, 0, out.data());
@@ -372,46 +432,48 @@ struct ab_transform
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, s));
 		++launches;
 	}
-	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp = nullptr) const
+	// twiddles of a domain (q: Q, else R)
+	const uint2 * wf(bool q) const { return tw(q ? WQ : WR); }
+	const uint2 * wv(bool q) const { return q ? nullptr : tw(WRI); }
+	RowJob rj(u32 * x, int mode, bool q, const u32 * xp = nullptr) const
 	{
-		RowJob j; std::memset(&j, 0, sizeof(j)); j.x = x; j.xp = xp; j.w = w; j.mode = mode; return j;
+		RowJob j; std::memset(&j, 0, sizeof(j)); j.x = x; j.xp = xp; j.w = wf(q); j.wi = wv(q); j.mode = mode; return j;
 	}
 	ColJob cj_norm(const u32 * in) const
 	{
 		ColJob j; std::memset(&j, 0, sizeof(j)); j.in = in; j.transformed = 0; j.a = 1; return j;
 	}
-	ColJob cj_tr(const u32 * in, const u32 * w_in, u32 a, int nega, const u32 * sub, int lower) const
+	ColJob cj_tr(const u32 * in, bool q, u32 a, const u32 * sub, int lower) const
 	{
 		ColJob j; std::memset(&j, 0, sizeof(j));
-		j.in = in; j.transformed = 1; j.w_in = w_in; j.a = a; j.nega = nega; j.sub = sub; j.lower = lower;
+		j.in = in; j.transformed = 1; j.w_in = wf(q); j.wi_in = wv(q); j.a = a; j.nega = q ? 1 : 0; j.sub = sub; j.lower = lower;
 		return j;
 	}
-	static void set_fwd(ColJob & j, u32 * q_out, const u32 * wq, u32 * r_out, const u32 * wr)
+	void set_fwd(ColJob & j, u32 * q_out, u32 * r_out) const
 	{
-		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wq : nullptr;
-		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wr : nullptr;
+		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wf(true) : nullptr;
+		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wf(false) : nullptr;
 	}
 
 	// full forward transform of a normal-form register in one or two domains
 	void full_forward(const u32 * src, u32 * dq, u32 * dr)
 	{
-		ColJob j = cj_norm(src); set_fwd(j, dq, b(WQ), dr, b(WR)); cols(j);
-		if (dq && dr) { RowJob a = rj(dq, ROW_FWD_ONLY, b(WQ)), c = rj(dr, ROW_FWD_ONLY, b(WR)); rows(a, &c); }
-		else if (dq) rows(rj(dq, ROW_FWD_ONLY, b(WQ)));
-		else rows(rj(dr, ROW_FWD_ONLY, b(WR)));
+		ColJob j = cj_norm(src); set_fwd(j, dq, dr); cols(j);
+		if (dq && dr) { RowJob a = rj(dq, ROW_FWD_ONLY, true), c = rj(dr, ROW_FWD_ONLY, false); rows(a, &c); }
+		else if (dq) rows(rj(dq, ROW_FWD_ONLY, true));
+		else rows(rj(dr, ROW_FWD_ONLY, false));
 	}
 
 	// reduceMMGW tail (transformGPU.h:523-538): m' = T_R Ninv mod R, +2,
 	// r' = m' N - T_Q mod Q.  AR1 holds the first forward levels of T_R.
 	void reduce_tail(const u32 * tq, u32 * out, bool want_prefwd, bool join_q = false)
 	{
-		rows(rj(b(AR1), ROW_MUL, b(WR), b(NIR)));
-		ColJob j1 = cj_tr(b(AR1), b(WR), 1, 0, nullptr, LOWER_R_ADD2); set_fwd(j1, b(AQ1), b(WQ), nullptr, nullptr); cols(j1);
-		rows(rj(b(AQ1), ROW_MUL, b(WQ), b(NQ)));
+		rows(rj(b(AR1), ROW_MUL, false, b(NIR)));
+		ColJob j1 = cj_tr(b(AR1), false, 1, nullptr, LOWER_R_ADD2); set_fwd(j1, b(AQ1), nullptr); cols(j1);
+		rows(rj(b(AQ1), ROW_MUL, true, b(NQ)));
 		if (join_q) CK(cudaStreamWaitEvent(st, ev_q, 0));
-		ColJob j2 = cj_tr(b(AQ1), b(WQ), 1, 1, tq, LOWER_Q); j2.out_norm = out;
-		j2.sub_big = (tq == b(TQ)) ? 1 : 0;     // T_Q of first_product holds exact coefficient values
-		if (want_prefwd) set_fwd(j2, b(AQ0), b(WQ), b(AR0), b(WR));
+		ColJob j2 = cj_tr(b(AQ1), true, 1, tq, LOWER_Q); j2.out_norm = out;
+		if (want_prefwd) set_fwd(j2, b(AQ0), b(AR0));
 		cols(j2);
 	}
 
@@ -424,9 +486,9 @@ struct ab_transform
 	// read in place of `a` (graph replays).
 	void first_product(u32 a, const u32 * xq, const u32 * xr, const u32 * mult = nullptr)
 	{
-		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, b(WQ), xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, b(WR), xr);
-		ColJob jq = cj_tr(b(AQ0), b(WQ), a, 1, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.out_big = 1; jq.mult = mult;
-		ColJob jr = cj_tr(b(AR0), b(WR), a, 0, nullptr, LOWER_NONE); set_fwd(jr, nullptr, nullptr, b(AR1), b(WR)); jr.mult = mult;
+		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, true, xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, false, xr);
+		ColJob jq = cj_tr(b(AQ0), true, a, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.mult = mult;
+		ColJob jr = cj_tr(b(AR0), false, a, nullptr, LOWER_NONE); set_fwd(jr, nullptr, b(AR1)); jr.mult = mult;
 		if (overlap)
 		{
 			CK(cudaEventRecord(ev_fork, st));
@@ -449,10 +511,15 @@ struct ab_transform
 		}
 	}
 
+	void prefwd_reg0()
+	{
+		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(AR0)); cols(j); }
+	}
+
 	// squareMMGW (transformGPU.h:556-568)
 	void square_mul(u32 a)
 	{
-		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		prefwd_reg0();
 		first_product(a, nullptr, nullptr);
 		reduce_tail(b(TQ), b(REG0), true, overlap);
 		prefwd = true;
@@ -496,7 +563,7 @@ struct ab_transform
 			cudaGraphDestroy(g);
 			CK(ei);
 		}
-		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		prefwd_reg0();
 		const int hi = mult_i;
 		CK(cudaEventSynchronize(mult_done[hi]));
 		std::memcpy(h_mult[hi], mults, G * sizeof(u32));
@@ -530,7 +597,7 @@ struct ab_transform
 	void mul(int dst, int src)
 	{
 		full_forward(b(src), b(OPQ), b(OPR));
-		{ ColJob j = cj_norm(b(dst)); set_fwd(j, b(AQ0), b(WQ), b(AR0), b(WR)); cols(j); }
+		{ ColJob j = cj_norm(b(dst)); set_fwd(j, b(AQ0), b(AR0)); cols(j); }
 		prefwd = false;
 		first_product(1, b(OPQ), b(OPR));
 		reduce_tail(b(TQ), b(dst), dst == REG0, overlap);
@@ -540,38 +607,58 @@ struct ab_transform
 	// conversion out of MMGW form into TMP (transformGPU.h:576-586)
 	void reduce_copy(int src)
 	{
-		ColJob j = cj_norm(b(src)); set_fwd(j, nullptr, nullptr, b(AR1), b(WR)); cols(j);
+		ColJob j = cj_norm(b(src)); set_fwd(j, nullptr, b(AR1)); cols(j);
 		reduce_tail(b(src), b(TMP), false);
 	}
 
 	void copy(int dst, int src)
 	{
 		if (dst == src) return;
-		CK(cudaMemcpyAsync(b(dst), b(src), (size_t)prm.K * n * 4, cudaMemcpyDeviceToDevice, st));
+		CK(cudaMemcpyAsync(b(dst), b(src), words_of(dst) * 4, cudaMemcpyDeviceToDevice, st));
 		if (dst == REG0) prefwd = false;
 	}
 
 	void upload(int buf, const u32 * src)
 	{
-		CK(cudaMemcpyAsync(b(buf), src, (size_t)prm.K * n * 4, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(buf), src, words_of(buf) * 4, cudaMemcpyHostToDevice, st));
 		CK(cudaStreamSynchronize(st));
 	}
-	void download(int buf, u32 * dst, size_t planes)
+	void download(int buf, u32 * dst, size_t words)
 	{
-		CK(cudaMemcpyAsync(dst, b(buf), planes * n * 4, cudaMemcpyDeviceToHost, st));
+		CK(cudaMemcpyAsync(dst, b(buf), words * 4, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
+	}
+
+	// the reference's register words (K planes) of a normal-form buffer, into XW
+	void export_words(int buf)
+	{
+		CK(launch_export(rc, b(buf), b(XW), (u32)n, st));
+		++launches;
+	}
+	// XW (the reference's register words) into a normal-form buffer; returns
+	// false when they are not a normal-form register
+	bool import_words(int buf)
+	{
+		CK(cudaMemsetAsync(d_flag, 0, sizeof(u32), st));
+		CK(launch_import(rc, b(XW), b(buf), (u32)n, d_flag, st));
+		++launches;
+		u32 bad = 0;
+		CK(cudaMemcpyAsync(&bad, d_flag, sizeof(u32), cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		if (buf == REG0) prefwd = false;
+		return bad == 0;
 	}
 
 	void get(int src, mpz_t z)
 	{
 		reduce_copy(src);
-		host.resize((size_t)prm.K * n);
-		download(TMP, host.data(), (size_t)prm.pck);
+		host.resize((size_t)AB_NW * n);
+		download(TMP, host.data(), (size_t)AB_NW * n);
 		decode(host.data(), z);
 	}
 
 	// host part of the set-up: parameters, geometry, R, N^-1 mod R, constants,
-	// and the register words of N, N^-1 and the MMGW form of 1
+	// and the exact values of N, N^-1 and the MMGW form of 1
 	struct Prepared
 	{
 		std::vector<u32> wN, wNinv, wOne;
@@ -581,14 +668,16 @@ struct ab_transform
 	{
 		mpz_set(N, Nin);
 		prm = forced ? *forced : select_params(N, a);
-		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31)
+		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31 ||
+		    prm.pck * prm.lbase > 80)
 			throw ab_error(AB_E_ARG, "invalid transform parameters");
 		if (!make_geometry(prm.ln, 0, geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length 2^" + std::to_string(prm.ln) + " is not supported (6 <= ln <= 20)");
 		n = (size_t)1 << prm.ln;
+		KP = prm.K + 1;
 		mpz_t R, Ninv; mpz_inits(R, Ninv, nullptr);
 		if (!compute_R_Ninv(N, prm, R, Ninv, factor)) { failed = true; mpz_clears(R, Ninv, nullptr); return; }
-		build_consts();
-		const size_t words = (size_t)prm.K * n;
+		build_consts(prm, geo, tc, rc);
+		const size_t words = (size_t)AB_NW * n;
 		pp.wN.resize(words); pp.wNinv.resize(words); pp.wOne.resize(words);
 		encode(N, pp.wN.data());
 		encode(Ninv, pp.wNinv.data());
@@ -611,6 +700,19 @@ struct ab_transform
 		CK(cudaStreamSynchronize(st));
 	}
 
+	// twiddle tables of the class (host), KP n words per table
+	static void twiddle_tables(const ab_params & prm, std::vector<uint2> & wr, std::vector<uint2> & wri, std::vector<uint2> & wq)
+	{
+		const size_t h = (size_t)1 << (prm.ln - 1);
+		const int KP = prm.K + 1;
+		wr.assign(KP * h, make_uint2(0, 0)); wri.assign(KP * h, make_uint2(0, 0)); wq.assign(KP * h, make_uint2(0, 0));
+		for (int k = 0; k < KP; ++k)
+		{
+			make_twiddles(&wr[k * h], &wri[k * h], prm.ln, k, false);
+			make_twiddles(&wq[k * h], nullptr, prm.ln, k, true);
+		}
+	}
+
 	void init(const mpz_t Nin, int32_t a, int dev, const ab_params * forced)
 	{
 		device = dev;
@@ -625,24 +727,32 @@ struct ab_transform
 		CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
 		CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
 		CK(cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming));
-		CK(cudaMalloc(&dmem, (size_t)NBUF * prm.K * n * 4));
-		CK(cudaMemsetAsync(dmem, 0, (size_t)NBUF * prm.K * n * 4, st));
-		for (int i = 0; i < NBUF; ++i) bufp[i] = dmem + (size_t)i * prm.K * n;
+		size_t total = 64;                   // the flag word, then the buffers (each 256-byte aligned)
+		size_t offs[NBUF];
+		for (int i = 0; i < NBUF; ++i) { offs[i] = total; total += (words_of(i) + 63) / 64 * 64; }
+		CK(cudaMalloc(&dmem, total * 4));
+		CK(cudaMemsetAsync(dmem, 0, total * 4, st));
+		d_flag = dmem;
+		for (int i = 0; i < NBUF; ++i) bufp[i] = dmem + offs[i];
 
-		host.assign((size_t)prm.K * n, 0);
-		std::vector<u32> wr((size_t)prm.K * n), wq((size_t)prm.K * n);
-		for (int k = 0; k < prm.K; ++k) { make_roots(&wr[(size_t)k * n], prm.ln, k, false); make_roots(&wq[(size_t)k * n], prm.ln, k, true); }
-		upload(WR, wr.data()); upload(WQ, wq.data());
+		host.assign((size_t)AB_NW * n, 0);
+		std::vector<uint2> wr, wri, wq;
+		twiddle_tables(prm, wr, wri, wq);
+		CK(cudaMemcpyAsync(b(WR), wr.data(), wr.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(WRI), wri.data(), wri.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(WQ), wq.data(), wq.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaStreamSynchronize(st));
 		setup_device(pp);
 	}
 };
 
 // ============================================================ batches
 // A size class (K, pck, ln) of `cap` candidates with stacked buffers: buffer
-// type i of slot s is at base[i] + s * words.  Each loaded slot is exposed as
-// an ab_transform view (set1 / copy / mul / get work unchanged on it); the
-// squarings of all slots run together (grid.z = slot) from a captured CUDA
-// graph whose per-step, per-slot multipliers are uploaded before each launch.
+// type i of slot s is at base[i] + s * (its words).  Each loaded slot is
+// exposed as an ab_transform view (set1 / copy / mul / get work unchanged on
+// it); the squarings of all slots run together (grid.z = slot) from a
+// captured CUDA graph whose per-step, per-slot multipliers are uploaded
+// before each launch.
 struct ab_batch
 {
 	int device = 0;
@@ -650,9 +760,11 @@ struct ab_batch
 	ab_params cls{};
 	Geometry geo{};
 	TConst tc{};
-	size_t n = 0, words = 0;
+	RefConst rc{};
+	size_t n = 0, w_ntt = 0, w_norm = 0;   // words of an NTT-form / normal-form buffer of one slot
 	int cap = 0, max_steps = 0;
 	u32 * mem = nullptr;
+	u32 * d_flag = nullptr;
 	u32 * base[ab_transform::NBUF] = {};
 	CandConst * d_cand = nullptr;
 	std::vector<CandConst> h_cand;
@@ -677,7 +789,10 @@ struct ab_batch
 		if (st) cudaStreamDestroy(st);
 	}
 
+	size_t slot_words(int i) const { return ab_transform::normal_buf(i) ? w_norm : w_ntt; }
 	u32 * ctrl(int step, int part) const { return d_ctrl + ((size_t)step * 3 + part) * cap; }
+	const uint2 * wf(bool q) const { return reinterpret_cast<const uint2 *>(base[q ? ab_transform::WQ : ab_transform::WR]); }
+	const uint2 * wv(bool q) const { return q ? nullptr : reinterpret_cast<const uint2 *>(base[ab_transform::WRI]); }
 
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
@@ -689,18 +804,25 @@ struct ab_batch
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, zl));
 	}
-	RowJob rj(u32 * x, int mode, const u32 * w, const u32 * xp, const u32 * act) const
+	RowJob rj(u32 * x, int mode, bool q, const u32 * xp, const u32 * act) const
 	{
 		RowJob j; std::memset(&j, 0, sizeof(j));
-		j.x = x; j.xp = xp; j.w = w; j.mode = mode; j.stride = words; j.active = act;
+		j.x = x; j.xp = xp; j.w = wf(q); j.wi = wv(q); j.mode = mode; j.stride = w_ntt; j.active = act;
 		return j;
 	}
-	ColJob cj(const u32 * in, bool tr, const u32 * w_in, const u32 * mult, int nega, const u32 * sub, int lower) const
+	ColJob cj(const u32 * in, bool tr, bool q, const u32 * mult, const u32 * sub, int lower) const
 	{
 		ColJob j; std::memset(&j, 0, sizeof(j));
-		j.in = in; j.transformed = tr ? 1 : 0; j.w_in = w_in; j.a = 1; j.mult = mult; j.nega = nega; j.sub = sub;
-		j.lower = lower; j.stride = words; j.cand = d_cand;
+		j.in = in; j.transformed = tr ? 1 : 0;
+		if (tr) { j.w_in = wf(q); j.wi_in = wv(q); j.nega = q ? 1 : 0; }
+		j.a = 1; j.mult = mult; j.sub = sub;
+		j.lower = lower; j.stride_ntt = w_ntt; j.stride_norm = w_norm; j.cand = d_cand;
 		return j;
+	}
+	void set_fwd(ColJob & j, u32 * q_out, u32 * r_out) const
+	{
+		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wf(true) : nullptr;
+		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wf(false) : nullptr;
 	}
 
 	// squareMMGW (transformGPU.h:556-568) for every slot, `steps` times
@@ -708,27 +830,26 @@ struct ab_batch
 	{
 		using T = ab_transform;
 		u32 * const aq0 = base[T::AQ0], * const ar0 = base[T::AR0], * const aq1 = base[T::AQ1], * const ar1 = base[T::AR1];
-		const u32 * wq = base[T::WQ], * wr = base[T::WR];
 		{
-			ColJob j = cj(base[T::REG0], false, nullptr, ctrl(0, 1), 0, nullptr, LOWER_NONE);
-			j.out_fwd[0] = aq0; j.w_out[0] = wq; j.out_fwd[1] = ar0; j.w_out[1] = wr;
+			ColJob j = cj(base[T::REG0], false, false, ctrl(0, 1), nullptr, LOWER_NONE);
+			set_fwd(j, aq0, ar0);
 			cols(j);
 		}
 		for (int s = 0; s < steps; ++s)
 		{
 			const u32 * mult = ctrl(s, 0), * act = ctrl(s, 1), * snap = ctrl(s, 2);
-			RowJob rq = rj(aq0, ROW_SQUARE, wq, nullptr, act), rr = rj(ar0, ROW_SQUARE, wr, nullptr, act);
+			RowJob rq = rj(aq0, ROW_SQUARE, true, nullptr, act), rr = rj(ar0, ROW_SQUARE, false, nullptr, act);
 			rows(rq, &rr);
-			ColJob jq = cj(aq0, true, wq, mult, 1, nullptr, LOWER_NONE); jq.out_norm = base[T::TQ]; jq.out_big = 1;
-			ColJob jr = cj(ar0, true, wr, mult, 0, nullptr, LOWER_NONE); jr.out_fwd[1] = ar1; jr.w_out[1] = wr;
+			ColJob jq = cj(aq0, true, true, mult, nullptr, LOWER_NONE); jq.out_norm = base[T::TQ];
+			ColJob jr = cj(ar0, true, false, mult, nullptr, LOWER_NONE); set_fwd(jr, nullptr, ar1);
 			cols(jq, &jr);
-			rows(rj(ar1, ROW_MUL, wr, base[T::NIR], act));
-			ColJob j1 = cj(ar1, true, wr, act, 0, nullptr, LOWER_R_ADD2); j1.out_fwd[0] = aq1; j1.w_out[0] = wq;
+			rows(rj(ar1, ROW_MUL, false, base[T::NIR], act));
+			ColJob j1 = cj(ar1, true, false, act, nullptr, LOWER_R_ADD2); set_fwd(j1, aq1, nullptr);
 			cols(j1);
-			rows(rj(aq1, ROW_MUL, wq, base[T::NQ], act));
-			ColJob j2 = cj(aq1, true, wq, act, 1, base[T::TQ], LOWER_Q); j2.sub_big = 1;
+			rows(rj(aq1, ROW_MUL, true, base[T::NQ], act));
+			ColJob j2 = cj(aq1, true, true, act, base[T::TQ], LOWER_Q);
 			j2.out_norm = base[T::REG0];
-			j2.out_fwd[0] = aq0; j2.w_out[0] = wq; j2.out_fwd[1] = ar0; j2.w_out[1] = wr;
+			set_fwd(j2, aq0, ar0);
 			j2.out_snap = base[T::SNAP]; j2.snap_flag = snap;
 			cols(j2);
 		}
@@ -918,11 +1039,13 @@ int ab_save_checkpoint(ab_transform * h, void * buf, size_t cap, size_t * writte
 		if (buf == nullptr || cap < need) throw ab_error(AB_E_CAPACITY, "checkpoint buffer too small");
 		u32 * o = static_cast<u32 *>(buf);
 		o[0] = (u32)K; o[1] = (u32)n;
-		// per prime k: plane k of Reg0 then plane k of Reg1 (transformGPU.h:626-641)
-		for (size_t k = 0; k < K; ++k)
+		// per prime k: plane k of Reg0 then plane k of Reg1 (transformGPU.h:626-641),
+		// the reference's register words
+		for (int r = 0; r < 2; ++r)
 		{
-			CK(cudaMemcpyAsync(o + 2 + 2 * k * n, h->b(ab_transform::REG0) + k * n, n * 4, cudaMemcpyDeviceToHost, h->st));
-			CK(cudaMemcpyAsync(o + 2 + 2 * k * n + n, h->b(ab_transform::REG1) + k * n, n * 4, cudaMemcpyDeviceToHost, h->st));
+			h->export_words(r == 0 ? ab_transform::REG0 : ab_transform::REG1);
+			for (size_t k = 0; k < K; ++k)
+				CK(cudaMemcpyAsync(o + 2 + 2 * k * n + r * n, h->b(ab_transform::XW) + k * n, n * 4, cudaMemcpyDeviceToHost, h->st));
 		}
 		CK(cudaStreamSynchronize(h->st));
 		if (written) *written = need;
@@ -937,13 +1060,15 @@ int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size)
 		if (buf == nullptr || size < 8) throw ab_error(AB_E_CHECKPOINT, "checkpoint too short");
 		const u32 * in = static_cast<const u32 *>(buf);
 		if (in[0] != K || in[1] != n || size < ab_checkpoint_size(h)) throw ab_error(AB_E_CHECKPOINT, "checkpoint does not match K or n");
-		for (size_t k = 0; k < K; ++k)
+		bool ok = true;
+		for (int r = 0; r < 2; ++r)
 		{
-			CK(cudaMemcpyAsync(h->b(ab_transform::REG0) + k * n, in + 2 + 2 * k * n, n * 4, cudaMemcpyHostToDevice, h->st));
-			CK(cudaMemcpyAsync(h->b(ab_transform::REG1) + k * n, in + 2 + 2 * k * n + n, n * 4, cudaMemcpyHostToDevice, h->st));
+			for (size_t k = 0; k < K; ++k)
+				CK(cudaMemcpyAsync(h->b(ab_transform::XW) + k * n, in + 2 + 2 * k * n + r * n, n * 4, cudaMemcpyHostToDevice, h->st));
+			ok = h->import_words(r == 0 ? ab_transform::REG0 : ab_transform::REG1) && ok;
 		}
-		CK(cudaStreamSynchronize(h->st));
 		h->prefwd = false;
+		if (!ok) throw ab_error(AB_E_CHECKPOINT, "checkpoint registers are not in normal form");
 	});
 }
 
@@ -961,7 +1086,8 @@ int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_wo
 	return guarded([&] {
 		need_ready(h);
 		if (!valid_reg(reg) || out == nullptr || cap_words < (size_t)h->prm.K * h->n) throw ab_error(AB_E_ARG, "bad arguments");
-		h->download((int)reg, out, (size_t)h->prm.K);
+		h->export_words((int)reg);
+		h->download(ab_transform::XW, out, (size_t)h->prm.K * h->n);
 	});
 }
 
@@ -970,8 +1096,8 @@ int ab_write_register(ab_transform * h, size_t reg, const uint32_t * in, size_t 
 	return guarded([&] {
 		need_ready(h);
 		if (!valid_reg(reg) || in == nullptr || nwords != (size_t)h->prm.K * h->n) throw ab_error(AB_E_ARG, "bad arguments");
-		h->upload((int)reg, in);
-		if (reg == 0) h->prefwd = false;
+		h->upload(ab_transform::XW, in);
+		if (!h->import_words((int)reg)) throw ab_error(AB_E_ARG, "the words are not a normal-form register");
 	});
 }
 
@@ -1045,28 +1171,49 @@ int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg, int32_t a)
 	return guarded([&] {
 		need_ready(h);
 		if (reg == nullptr || a < 1) throw ab_error(AB_E_ARG, "null register or multiplier a < 1");
-		const size_t words = (size_t)h->prm.K * h->n;
-		if (words > AB_NOALLOC_MAX_WORDS)
-			throw ab_error(AB_E_CAPACITY, "ab_square_mul_noalloc: K*n = " + std::to_string(words) +
-				" words exceeds the static scratch limit of " + std::to_string(AB_NOALLOC_MAX_WORDS) + " words per register");
+		const size_t n = h->n, ntt_words = (size_t)h->KP * n;
+		if (ntt_words > AB_NOALLOC_MAX_WORDS || 2 * AB_NW * n > AB_NOALLOC_MAX_WORDS)
+			throw ab_error(AB_E_CAPACITY, "ab_square_mul_noalloc: NTT length 2^" + std::to_string(h->prm.ln) +
+				" exceeds the static scratch (at most 2^16 words per prime, " + std::to_string(AB_NOALLOC_MAX_WORDS) + " words per region)");
 		u32 * const s = (h->noalloc != nullptr) ? h->noalloc : noalloc_scratch(h->device);
 		u32 * const aq0 = s, * const ar0 = s + AB_NOALLOC_MAX_WORDS, * const aq1 = s + 2 * AB_NOALLOC_MAX_WORDS;
 		u32 * const ar1 = s + 3 * AB_NOALLOC_MAX_WORDS, * const tq = s + 4 * AB_NOALLOC_MAX_WORDS;
+		u32 * const x = tq + AB_NW * n, * const flag = s + 5 * AB_NOALLOC_MAX_WORDS;
 		using T = ab_transform;
-		const u32 * wq = h->b(T::WQ), * wr = h->b(T::WR);
+		// the caller's register words -> exact values in the scratch, then
 		// squareMMGW (transformGPU.h:556-568) with every intermediate in the
-		// static scratch: each scratch word is written before it is read
-		// within the call, so nothing needs clearing between calls
-		ColJob j0 = h->cj_norm(reg); T::set_fwd(j0, aq0, wq, ar0, wr); h->cols(j0);
-		RowJob rq = h->rj(aq0, ROW_SQUARE, wq), rr = h->rj(ar0, ROW_SQUARE, wr);
+		// static scratch, then back to the caller's register words.  Each
+		// scratch word is written before it is read within the call, so
+		// nothing needs clearing between calls.
+		CK(launch_import(h->rc, reg, x, (u32)n, flag, h->st));
+		ColJob j0 = h->cj_norm(x); h->set_fwd(j0, aq0, ar0); h->cols(j0);
+		RowJob rq = h->rj(aq0, ROW_SQUARE, true), rr = h->rj(ar0, ROW_SQUARE, false);
 		h->rows(rq, &rr);
-		ColJob jq = h->cj_tr(aq0, wq, (u32)a, 1, nullptr, LOWER_NONE); jq.out_norm = tq;
-		ColJob jr = h->cj_tr(ar0, wr, (u32)a, 0, nullptr, LOWER_NONE); T::set_fwd(jr, nullptr, nullptr, ar1, wr);
+		ColJob jq = h->cj_tr(aq0, true, (u32)a, nullptr, LOWER_NONE); jq.out_norm = tq;
+		ColJob jr = h->cj_tr(ar0, false, (u32)a, nullptr, LOWER_NONE); h->set_fwd(jr, nullptr, ar1);
 		h->cols(jq, &jr);
-		h->rows(h->rj(ar1, ROW_MUL, wr, h->b(T::NIR)));
-		ColJob j1 = h->cj_tr(ar1, wr, 1, 0, nullptr, LOWER_R_ADD2); T::set_fwd(j1, aq1, wq, nullptr, nullptr); h->cols(j1);
-		h->rows(h->rj(aq1, ROW_MUL, wq, h->b(T::NQ)));
-		ColJob j2 = h->cj_tr(aq1, wq, 1, 1, tq, LOWER_Q); j2.out_norm = reg; h->cols(j2);
+		h->rows(h->rj(ar1, ROW_MUL, false, h->b(T::NIR)));
+		ColJob j1 = h->cj_tr(ar1, false, 1, nullptr, LOWER_R_ADD2); h->set_fwd(j1, aq1, nullptr); h->cols(j1);
+		h->rows(h->rj(aq1, ROW_MUL, true, h->b(T::NQ)));
+		ColJob j2 = h->cj_tr(aq1, true, 1, tq, LOWER_Q); j2.out_norm = x; h->cols(j2);
+		CK(launch_export(h->rc, x, reg, (u32)n, h->st));
+		h->launches += 2;
+	});
+}
+
+int ab_inject_word(ab_transform * h, size_t reg, size_t index, int32_t delta)
+{
+	return guarded([&] {
+		need_ready(h);
+		if (!valid_reg(reg)) throw ab_error(AB_E_ARG, "register index");
+		u32 * const w = h->b((int)reg) + index % (AB_NW * h->n);
+		u32 v = 0;
+		CK(cudaMemcpyAsync(&v, w, 4, cudaMemcpyDeviceToHost, h->st));
+		CK(cudaStreamSynchronize(h->st));
+		v += (u32)delta;
+		CK(cudaMemcpyAsync(w, &v, 4, cudaMemcpyHostToDevice, h->st));
+		CK(cudaStreamSynchronize(h->st));
+		if (reg == 0) h->prefwd = false;
 	});
 }
 
@@ -1074,31 +1221,43 @@ int ab_diag_forward(ab_transform * h, int domain, const uint32_t * in, uint32_t 
 {
 	return guarded([&] {
 		need_ready(h);
-		h->upload(ab_transform::TMP, in);
-		if (domain) h->full_forward(h->b(ab_transform::TMP), h->b(ab_transform::AQ1), nullptr);
-		else h->full_forward(h->b(ab_transform::TMP), nullptr, h->b(ab_transform::AQ1));
-		h->download(ab_transform::AQ1, out, (size_t)h->prm.K);
+		using T = ab_transform;
+		h->upload(T::XW, in);
+		if (!h->import_words(T::TMP)) throw ab_error(AB_E_ARG, "input is not a normal-form register");
+		if (domain) h->full_forward(h->b(T::TMP), h->b(T::AQ1), nullptr);
+		else h->full_forward(h->b(T::TMP), nullptr, h->b(T::AQ1));
+		h->download(T::AQ1, out, (size_t)h->KP * h->n);
+		h->prefwd = false;
 	});
 }
 
-int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * xp, uint32_t a,
+int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * y, uint32_t a,
 	const uint32_t * sub, int lower_mode, uint32_t * out)
 {
 	return guarded([&] {
 		need_ready(h);
 		using T = ab_transform;
-		const u32 * w = h->b(domain ? T::WQ : T::WR);
-		h->upload(T::TMP, in);
-		if (xp) h->upload(T::OPQ, xp);
-		if (sub) h->upload(T::OPR, sub);
+		const bool q = domain != 0;
+		auto load = [&](const uint32_t * words, int buf) {
+			h->upload(T::XW, words);
+			if (!h->import_words(buf)) throw ab_error(AB_E_ARG, "input is not a normal-form register");
+		};
+		load(in, T::TMP);
+		if (y)
+		{
+			load(y, T::SNAP);
+			h->full_forward(h->b(T::SNAP), q ? h->b(T::OPQ) : nullptr, q ? nullptr : h->b(T::OPR));
+		}
+		if (sub) load(sub, T::TQ);
 		ColJob j = h->cj_norm(h->b(T::TMP));
-		if (domain) T::set_fwd(j, h->b(T::AQ1), w, nullptr, nullptr); else T::set_fwd(j, nullptr, nullptr, h->b(T::AQ1), w);
+		if (q) h->set_fwd(j, h->b(T::AQ1), nullptr); else h->set_fwd(j, nullptr, h->b(T::AQ1));
 		h->cols(j);
-		h->rows(h->rj(h->b(T::AQ1), xp ? ROW_MUL : ROW_SQUARE, w, xp ? h->b(T::OPQ) : nullptr));
-		ColJob c = h->cj_tr(h->b(T::AQ1), w, a, domain ? 1 : 0, sub ? h->b(T::OPR) : nullptr, lower_mode);
+		h->rows(h->rj(h->b(T::AQ1), y ? ROW_MUL : ROW_SQUARE, q, y ? h->b(q ? T::OPQ : T::OPR) : nullptr));
+		ColJob c = h->cj_tr(h->b(T::AQ1), q, a, sub ? h->b(T::TQ) : nullptr, lower_mode);
 		c.out_norm = h->b(T::TMP);
 		h->cols(c);
-		h->download(T::TMP, out, (size_t)h->prm.K);
+		h->export_words(T::TMP);
+		h->download(T::XW, out, (size_t)h->prm.K * h->n);
 		h->prefwd = false;
 	});
 }
@@ -1106,8 +1265,11 @@ int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uin
 
 size_t ab_batch_slot_bytes(const ab_params * cls)
 {
-	if (cls == nullptr) return 0;
-	return (size_t)(ab_transform::WR) * cls->K * ((size_t)1 << cls->ln) * 4;
+	if (cls == nullptr || cls->K < 2 || cls->K > 5) return 0;
+	const size_t n = (size_t)1 << cls->ln, KP = (size_t)cls->K + 1;
+	size_t w = 0;
+	for (int i = 0; i < ab_transform::NSLOT; ++i) w += ab_transform::normal_buf(i) ? AB_NW * n : KP * n;
+	return w * 4;
 }
 
 int ab_batch_create(int device, const ab_params * cls, int capacity, int max_steps, ab_batch ** out)
@@ -1120,19 +1282,29 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 		b = new ab_batch();
 		b->device = device; b->cls = *cls; b->cap = capacity; b->max_steps = max_steps;
 		if (!make_geometry(cls->ln, 0, b->geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length not supported");
-		b->n = (size_t)1 << cls->ln; b->words = (size_t)cls->K * b->n;
+		b->n = (size_t)1 << cls->ln;
+		b->w_ntt = (size_t)(cls->K + 1) * b->n; b->w_norm = (size_t)AB_NW * b->n;
 		CK(cudaSetDevice(device));
 		CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
-		const size_t per = (size_t)ab_transform::WR;          // per-slot buffer types
-		CK(cudaMalloc(&b->mem, (per * capacity + 2) * b->words * 4));
-		CK(cudaMemsetAsync(b->mem, 0, (per * capacity + 2) * b->words * 4, b->st));
-		for (size_t i = 0; i < per; ++i) b->base[i] = b->mem + i * capacity * b->words;
-		b->base[ab_transform::WR] = b->mem + per * capacity * b->words;
-		b->base[ab_transform::WQ] = b->base[ab_transform::WR] + b->words;
-		std::vector<u32> wr(b->words), wq(b->words);
-		for (int k = 0; k < cls->K; ++k) { make_roots(&wr[(size_t)k * b->n], cls->ln, k, false); make_roots(&wq[(size_t)k * b->n], cls->ln, k, true); }
-		CK(cudaMemcpyAsync(b->base[ab_transform::WR], wr.data(), b->words * 4, cudaMemcpyHostToDevice, b->st));
-		CK(cudaMemcpyAsync(b->base[ab_transform::WQ], wq.data(), b->words * 4, cudaMemcpyHostToDevice, b->st));
+		// the flag word, the per-slot buffers (slot-major within each type), then
+		// the shared buffers: the reference words XW and the twiddle tables
+		size_t total = 64, offs[ab_transform::NBUF];
+		for (int i = 0; i < ab_transform::NBUF; ++i)
+		{
+			offs[i] = total;
+			const size_t w = (i < ab_transform::NSLOT) ? b->slot_words(i) * capacity
+			               : (i == ab_transform::XW) ? (size_t)cls->K * b->n : b->w_ntt;
+			total += (w + 63) / 64 * 64;
+		}
+		CK(cudaMalloc(&b->mem, total * 4));
+		CK(cudaMemsetAsync(b->mem, 0, total * 4, b->st));
+		b->d_flag = b->mem;
+		for (int i = 0; i < ab_transform::NBUF; ++i) b->base[i] = b->mem + offs[i];
+		std::vector<uint2> wr, wri, wq;
+		ab_transform::twiddle_tables(*cls, wr, wri, wq);
+		CK(cudaMemcpyAsync(b->base[ab_transform::WR], wr.data(), wr.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
+		CK(cudaMemcpyAsync(b->base[ab_transform::WRI], wri.data(), wri.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
+		CK(cudaMemcpyAsync(b->base[ab_transform::WQ], wq.data(), wq.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
 		CK(cudaMalloc(&b->d_cand, sizeof(CandConst) * capacity));
 		b->h_cand.assign(capacity, CandConst{});
 		for (auto & c : b->h_cand) c.lbase = 2;
@@ -1146,12 +1318,9 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 			CK(cudaEventRecord(b->ctrl_done[i], b->st));
 		}
 		b->views.assign(capacity, nullptr);
-		// TConst of the class (digit constants come from d_cand)
-		ab_transform probe_t;
-		probe_t.prm = *cls; probe_t.prm.lbase = 17; probe_t.n = b->n; probe_t.geo = b->geo;
-		probe_t.build_consts();
-		b->tc = probe_t.tc;
-		probe_t.view = true;
+		// constants of the class (the digit size comes from d_cand)
+		ab_params p = *cls; p.lbase = 17;
+		ab_transform::build_consts(p, b->geo, b->tc, b->rc);
 		// kernel attributes before any capture
 		RowJobs rjs{}; ColJobs cjs{};
 		CK(launch_rowpass(b->geo, b->tc, rjs, 1, b->st, 0));
@@ -1201,6 +1370,18 @@ void batch_prepare(int count, const uint64_t * const * Nl, const size_t * nlimbs
 	for (int i = 0; i < count; ++i) if (code[i] != AB_OK) throw ab_error(code[i], err[i]);
 }
 
+// A view's buffers: the slot's part of each per-slot buffer type, and the
+// batch's shared buffers and stream.
+void batch_attach(ab_batch * b, ab_transform * v, int slot)
+{
+	v->device = b->device; v->st = b->st; v->overlap = false;
+	v->KP = b->cls.K + 1;
+	v->d_flag = b->d_flag;
+	for (int i = 0; i < ab_transform::NSLOT; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->slot_words(i);
+	for (int i = ab_transform::NSLOT; i < ab_transform::NBUF; ++i) v->bufp[i] = b->base[i];
+	v->host.assign(b->w_norm, 0);
+}
+
 // Device part: the slot's buffers, the transforms of N and N^-1, the constants
 // of its digit size; the view then owns the slot.
 void batch_install(ab_batch * b, int slot, std::unique_ptr<ab_transform> & vp, const ab_transform::Prepared & pp)
@@ -1210,19 +1391,14 @@ void batch_install(ab_batch * b, int slot, std::unique_ptr<ab_transform> & vp, c
 		throw ab_error(AB_E_ARG, "N does not belong to this size class");
 	delete b->views[slot];
 	b->views[slot] = nullptr;
-	v->device = b->device; v->st = b->st; v->overlap = false;
+	batch_attach(b, v, slot);
 	v->noalloc = noalloc_scratch(b->device);
 	v->use_geometry(b->geo);             // the batch's split, which the autotuner may have changed
-	for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)slot * b->words;
-	v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
-	v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
 	if (!v->failed)
 	{
-		v->host.assign(b->words, 0);
 		v->setup_device(pp);
 		CandConst & c = b->h_cand[slot];
 		c.lbase = v->prm.lbase;
-		for (int k = 0; k < AB_MAXK; ++k) { c.rbase[k] = v->tc.rbase[k]; c.rbase_pck[k] = v->tc.rbase_pck[k]; }
 		CK(cudaMemcpyAsync(b->d_cand + slot, &c, sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
 		CK(cudaStreamSynchronize(b->st));
 	}
@@ -1274,15 +1450,11 @@ int ab_batch_clone(ab_batch * b, int dst, int src)
 		ab_transform * v = new ab_transform();
 		v->view = true;
 		mpz_set(v->N, s->N); mpz_set(v->factor, s->factor);
-		v->prm = s->prm; v->n = s->n; v->geo = s->geo; v->tc = s->tc; v->failed = s->failed;
-		v->device = b->device; v->st = b->st; v->overlap = false;
+		v->prm = s->prm; v->n = s->n; v->geo = s->geo; v->tc = s->tc; v->rc = s->rc; v->failed = s->failed;
+		batch_attach(b, v, dst);
 		v->noalloc = s->noalloc;
-		v->host.assign(b->words, 0);
-		for (int i = 0; i < ab_transform::WR; ++i) v->bufp[i] = b->base[i] + (size_t)dst * b->words;
-		v->bufp[ab_transform::WR] = b->base[ab_transform::WR];
-		v->bufp[ab_transform::WQ] = b->base[ab_transform::WQ];
-		for (int i = 0; i < ab_transform::WR; ++i)
-			CK(cudaMemcpyAsync(v->bufp[i], s->bufp[i], b->words * 4, cudaMemcpyDeviceToDevice, b->st));
+		for (int i = 0; i < ab_transform::NSLOT; ++i)
+			CK(cudaMemcpyAsync(v->bufp[i], s->bufp[i], b->slot_words(i) * 4, cudaMemcpyDeviceToDevice, b->st));
 		b->h_cand[dst] = b->h_cand[src];
 		CK(cudaMemcpyAsync(b->d_cand + dst, &b->h_cand[dst], sizeof(CandConst), cudaMemcpyHostToDevice, b->st));
 		CK(cudaStreamSynchronize(b->st));

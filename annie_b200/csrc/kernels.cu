@@ -1,43 +1,28 @@
 // NTT passes of the modular-squaring engine, sm_100a.
 //
 // Mathematics (reference: ocl/kernel.cl and src/transformGPU.h of galloty/annie):
-// a register holds, per prime p_k, n = 2^ln residues.  The forward transform
-// is LN-1 radix-2 levels; the level with S polynomials maps each block of
-// 2m = n/S coefficients mod (x^2m - c^2) to mod (x^m - c) and (x^m + c) with
-// c = w[S + j] (j = block index, twiddle table in bit-reversed order,
-// transformGPU.h:117-160).  The very first level takes plain residues and
-// leaves Montgomery residues (lower half times rsq, upper half times
-// w[0] = Montgomery(w[1]); kernel.cl:286-290).  The product of the resulting
-// degree-1 polynomials is taken mod (x^2 -+ w[n/4 + q/2]) (kernel.cl:230-256),
-// and the inverse levels undo the forward ones with the inverse twiddles
-// (kernel.cl:218-228).  All values are canonical residues, so the results are
-// bit-identical to the reference whatever the order of the butterflies.
+// per transform prime p_k, a register is n = 2^ln values.  The forward
+// transform is LN-1 radix-2 levels; the level with S polynomials maps each
+// block of 2m = n/S coefficients mod (x^2m - c^2) to mod (x^m - c) and
+// (x^m + c) with c = w[S + j] (j = block index, twiddle table in bit-reversed
+// order, transformGPU.h:117-160).  The product of the resulting degree-1
+// polynomials is taken mod (x^2 -+ w[n/4 + q/2]) (kernel.cl:230-256), and the
+// inverse levels undo the forward ones.  The transform primes are below 2^30,
+// so values stay lazily reduced ([0, 4p) forward, [0, 2p) inverse; see
+// arith.cuh) and every butterfly is one Shoup product and three adds.  Only
+// the exact coefficient values that the carry produces are visible outside,
+// and they do not depend on the primes or the order of the butterflies.
 //
 // This file splits the n coefficients 2-D (row*R + col): the column pass owns
-// the first LA levels (all H rows of 32 adjacent columns, all K primes, in
+// the first LA levels (all H rows of 32 adjacent columns, all KP primes, in
 // shared memory) and the row pass owns the last LB levels (one row of one
-// prime per CTA, 32 coefficients per thread in registers).
+// prime per CTA, 16 coefficients per thread in registers).
 #include <atomic>
 
 #include "kernels.h"
 
 namespace ab
 {
-
-// ---------------------------------------------------------------- butterflies
-__device__ __forceinline__ void fwd_bfly(u32 & x0, u32 & x1, u32 w, u32 wq, u32 p)
-{
-	const u32 t = mont_mul_c(x1, w, wq, p);
-	x1 = sub_mod(x0, t, p);
-	x0 = add_mod(x0, t, p);
-}
-
-__device__ __forceinline__ void inv_bfly(u32 & x0, u32 & x1, u32 wi, u32 wiq, u32 p)
-{
-	const u32 t = sub_mod(x0, x1, p);
-	x0 = add_mod(x0, x1, p);
-	x1 = mont_mul_c(t, wi, wiq, p);
-}
 
 // ================================================================ row pass
 // A CTA transforms one row (R = 2^(LB+1) words) of one prime: levels
@@ -49,21 +34,20 @@ __device__ __forceinline__ void inv_bfly(u32 & x0, u32 & x1, u32 wi, u32 wiq, u3
 // Stage loops are rolled (runtime bit positions) to keep the code small.
 constexpr int RP_EPT = 16;
 
-// element of a stage with S group bits at bit b; the other bits come from
-// o = tid + T*x (x selects one of the 16 / 2^S groups of the thread)
-__device__ __forceinline__ u32 rp_elem(u32 tid, u32 T, int x, int S, int b, int g)
+// Twiddles of the row pass: the forward levels read w; the inverse levels
+// read the -w^-1 table wi (domain R) or, for domain Q (wi == null), the
+// forward table at the mirrored position of the level: the level with s
+// polynomials holds indices [s, 2s), and index i mirrors to 3s - 1 - i.
+struct RowTw
 {
-	const u32 o = tid + T * (u32)x;
-	return (o & ((1u << b) - 1)) | ((u32)g << b) | ((o >> b) << (b + S));
-}
+	const uint2 * w;
+	const uint2 * wi;
+	u32 H;
+};
 
-// two pad words per 32: conflict-free for every stage layout, including the
-// last one (lanes 2m, 2m+1 at elements 32m + {0,1} + 2g)
-__device__ __forceinline__ u32 rp_pad(u32 e) { return e + ((e >> 5) << 1); }
-
-template <int S, bool INV, bool SAVE>
-__device__ __forceinline__ void rp_radix(u32 (&v)[RP_EPT], u32 tid, u32 T, int b, int LB, const u32 * __restrict__ w,
-	u32 Hr, u32 p, u32 q, u32 (&w1)[8], u32 (&w1q)[8])
+template <int S, bool INV>
+__device__ __forceinline__ void rp_radix(u32 (&v)[RP_EPT], u32 tid, u32 T, int b, int LB, const RowTw & tw,
+	u32 Hr, u32 p, u32 p2)
 {
 	constexpr int G = RP_EPT >> S;
 #pragma unroll
@@ -75,19 +59,20 @@ __device__ __forceinline__ void rp_radix(u32 (&v)[RP_EPT], u32 tid, u32 T, int b
 		{
 			const int s = INV ? ss : (S - 1 - ss);
 			const int t = LB - b - s;
-			const u32 * __restrict__ wl = w + ((Hr << t) + (ohi << (S - 1 - s)));
+			const u32 i0 = (Hr << t) + (ohi << (S - 1 - s));
 #pragma unroll
 			for (int jh = 0; jh < (1 << (S - 1 - s)); ++jh)
 			{
-				const u32 wv = __ldg(wl + jh);
-				const u32 wq = wv * q;
-				if (SAVE && s == 0) { w1[jh] = wv; w1q[jh] = wq; }
+				uint2 wv;
+				if (!INV) wv = __ldg(tw.w + i0 + jh);
+				else if (tw.wi != nullptr) wv = __ldg(tw.wi + i0 + jh);
+				else wv = __ldg(tw.w + (3u * (tw.H << t) - 1u - (i0 + jh)));
 #pragma unroll
 				for (int gl = 0; gl < (1 << s); ++gl)
 				{
 					const int g = x * (1 << S) + (jh << (s + 1)) + gl;
-					if (INV) inv_bfly(v[g], v[g + (1 << s)], wv, wq, p);
-					else fwd_bfly(v[g], v[g + (1 << s)], wv, wq, p);
+					if (INV) inv_bf(v[g], v[g + (1 << s)], wv.x, wv.y, p, p2);
+					else fwd_bf(v[g], v[g + (1 << s)], wv.x, wv.y, p, p2);
 				}
 			}
 		}
@@ -97,6 +82,8 @@ __device__ __forceinline__ void rp_radix(u32 (&v)[RP_EPT], u32 tid, u32 T, int b
 // Stage addressing: the 2^S words of a group are e0 + g 2^b.  In the padded
 // shared layout they are pad(e0) + g D with D = 2^b + 2^(b-4) for b >= 5, and
 // D = 2 for the last stage (b = 1, the group stays inside one 32-word block).
+__device__ __forceinline__ u32 rp_pad(u32 e) { return e + ((e >> 5) << 1); }
+
 __device__ __forceinline__ u32 rp_base(u32 tid, u32 T, int x, int S, int b)
 {
 	const u32 o = tid + T * (u32)x;
@@ -157,54 +144,62 @@ __device__ __forceinline__ void rp_store_global(const u32 (&v)[RP_EPT], u32 * __
 // Pointwise product of the degree-1 polynomials (x0, x1) mod (x^2 -+ c):
 // lane 2m holds the x0 of the thread pair's 16 polynomials, lane 2m+1 the x1.
 // Each lane computes 8 whole products (even lane: slots 0..7, odd: 8..15).
+// Inputs: [0, 4p) from the forward levels, the other operand in [0, 2p);
+// every product is a Montgomery product (a factor 2^-32 that the carry's CRT
+// weights remove); outputs in [0, 2p) for the inverse levels.
+// w1: the 8 twiddles of the thread pair's last forward level (just read by
+// the forward stage, so an L1 hit), which are the polynomials' c.
 __device__ __forceinline__ void rp_pointwise(u32 (&v)[RP_EPT], const u32 * __restrict__ xp, bool is_mul, u32 tid, u32 NT,
-	const u32 (&w1)[8], const u32 (&w1q)[8], u32 p, u32 q)
+	const uint2 * __restrict__ w1, u32 p, u32 p2, u32 pinv)
 {
 	// tid: virtual thread (its 16 words are the last-stage elements
 	// 32*(tid>>1) + (tid&1) + 2g); NT: physical threads of the CTA (warp mask)
 	const bool odd = (tid & 1) != 0;
 	const unsigned mask = (NT >= 32) ? 0xffffffffu : ((1u << NT) - 1);
-	u32 pv[RP_EPT];
-	if (is_mul)
-	{
-#pragma unroll
-		for (int i = 0; i < RP_EPT; ++i) pv[i] = __ldg(&xp[(tid & 1) + 2 * i + ((tid >> 1) << 5)]);
-	}
+	const u32 * __restrict__ xq = is_mul ? xp + (tid & 1) + ((tid >> 1) << 5) : nullptr;
 #pragma unroll
 	for (int i = 0; i < 8; ++i)
 	{
 		const u32 r = __shfl_xor_sync(mask, odd ? v[i] : v[8 + i], 1);
-		const u32 x0 = odd ? r : v[i], x1 = odd ? v[8 + i] : r;
+		const u32 x0 = red2(odd ? r : v[i], p2), x1 = red2(odd ? v[8 + i] : r, p2);
 		const int slot = odd ? 8 + i : i;   // polynomial slot; parity = sign
-		const u32 cw = odd ? w1[4 + (i >> 1)] : w1[i >> 1];
-		const u32 cq = odd ? w1q[4 + (i >> 1)] : w1q[i >> 1];
-		u32 t, y0, y1;
+		const uint2 cwp = __ldg(w1 + (odd ? 4 + (i >> 1) : (i >> 1)));
+		const u32 cw = cwp.x, cs = cwp.y;
+		u32 y0, y1, t;
 		if (is_mul)
 		{
-			const u32 rp2 = __shfl_xor_sync(mask, odd ? pv[i] : pv[8 + i], 1);
-			const u32 p0 = odd ? rp2 : pv[i], p1 = odd ? pv[8 + i] : rp2;
-			t = mont_mul_c(mont_mul(x1, p1, p, q), cw, cq, p);
-			y1 = add_mod(mont_mul(x0, p1, p, q), mont_mul(p0, x1, p, q), p);
-			y0 = mont_mul(x0, p0, p, q);
+			const u32 pa = __ldg(xq + 2 * i), pb = __ldg(xq + 2 * (8 + i));
+			const u32 rp2 = __shfl_xor_sync(mask, odd ? pa : pb, 1);
+			const u32 p0 = odd ? rp2 : pa, p1 = odd ? pb : rp2;
+			t = shoup(mont(x1, p1, p, pinv), cw, cs, p);
+			y1 = red2(mont(x0, p1, p, pinv) + mont(x1, p0, p, pinv), p2);
+			y0 = mont(x0, p0, p, pinv);
 		}
 		else
 		{
-			t = mont_mul_c(mont_mul(x1, x1, p, q), cw, cq, p);
-			y1 = mont_mul(add_mod(x0, x0, p), x1, p, q);
-			y0 = mont_mul(x0, x0, p, q);
+			t = shoup(mont(x1, x1, p, pinv), cw, cs, p);
+			y1 = mont(red2(x0 + x0, p2), x1, p, pinv);
+			y0 = mont(x0, x0, p, pinv);
 		}
-		y0 = ((slot & 1) == 0) ? add_mod(y0, t, p) : sub_mod(y0, t, p);
+		y0 = red2(((slot & 1) == 0) ? y0 + t : y0 - t + p2, p2);
 		const u32 r2 = __shfl_xor_sync(mask, odd ? y0 : y1, 1);
 		if (odd) { v[8 + i] = y1; v[i] = r2; }
 		else { v[i] = y0; v[8 + i] = r2; }
 	}
 }
 
+template <int N>
+__device__ __forceinline__ void reduce_all(u32 (&v)[N], u32 p2)
+{
+#pragma unroll
+	for (int i = 0; i < N; ++i) v[i] = red2(v[i], p2);
+}
+
 // Physical threads of a row-pass CTA: 16 words per virtual thread, at most
 // 256 threads, each running R / (16 * threads) rounds per stage.  The kernel
 // is compiled for 4 CTAs per SM (at most 64 registers), so that the Q- and
 // R-domain row passes, which run side by side on two streams, are resident
-// together (measured: 4 % faster per squaring at 33.2 M bits than 3 per SM).
+// together.
 template <int LOG_R>
 struct RowCfg
 {
@@ -229,15 +224,18 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 	if (J.active != nullptr && J.active[cand] == 0u) return;
 	const size_t cofs = (size_t)cand * J.stride;
 	const u32 k = blockIdx.x / c.H, r = blockIdx.x - k * c.H;
-	const u32 p = c.p[k], q = c.q[k];
+	const u32 p = c.p[k], p2 = 2 * p, pinv = c.pinv[k];
 	u32 * __restrict__ x = J.x + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
-	const u32 * __restrict__ w = J.w + (size_t)k * c.n;
-	const u32 * __restrict__ wi = w + (c.n >> 1);
+	RowTw tw;
+	tw.w = J.w + (size_t)k * (c.n >> 1);
+	tw.wi = (J.wi != nullptr) ? J.wi + (size_t)k * (c.n >> 1) : nullptr;
+	tw.H = c.H;
 	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
 	const u32 Hr = c.H + r;
 	const u32 tid = threadIdx.x;
 	u32 v[RP_EPT];
-	u32 w1[8], w1q[8];
+	// twiddles of the last forward level of virtual thread vt: the c of its polynomials
+	auto w1 = [&](u32 vt) { return tw.w + (Hr << (LB - 1)) + ((vt >> 1) << 3); };
 
 	if constexpr (NS == 0)
 	{
@@ -246,12 +244,13 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 		{
 			const u32 vt = tid + rr * NT;
 			rp_load_global<4>(v, x, vt, T, 1);
-			rp_radix<4, false, true>(v, vt, T, 1, LB, w, Hr, p, q, w1, w1q);
+			rp_radix<4, false>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			if (J.mode != ROW_FWD_ONLY)
 			{
-				rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1, w1q, p, q);
-				rp_radix<4, true, false>(v, vt, T, 1, LB, wi, Hr, p, q, w1, w1q);
+				rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1(vt), p, p2, pinv);
+				rp_radix<4, true>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			}
+			else reduce_all(v, p2);
 			rp_store_global<4>(v, x, vt, T, 1);
 		}
 		return;
@@ -264,7 +263,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 		{
 			const u32 vt = tid + rr * NT;
 			rp_load_global<S0>(v, x, vt, T, B0);
-			rp_radix<S0, false, false>(v, vt, T, B0, LB, w, Hr, p, q, w1, w1q);
+			rp_radix<S0, false>(v, vt, T, B0, LB, tw, Hr, p, p2);
 			rp_store_smem<S0>(v, sm, vt, T, B0);
 		}
 		int b = B0;
@@ -278,7 +277,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 			{
 				const u32 vt = tid + rr * NT;
 				rp_load_smem<4>(v, sm, vt, T, b);
-				rp_radix<4, false, false>(v, vt, T, b, LB, w, Hr, p, q, w1, w1q);
+				rp_radix<4, false>(v, vt, T, b, LB, tw, Hr, p, p2);
 				rp_store_smem<4>(v, sm, vt, T, b);
 			}
 		}
@@ -290,14 +289,15 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 		{
 			const u32 vt = tid + rr * NT;
 			rp_load_smem<4>(v, sm, vt, T, 1);
-			rp_radix<4, false, true>(v, vt, T, 1, LB, w, Hr, p, q, w1, w1q);
+			rp_radix<4, false>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			if (J.mode == ROW_FWD_ONLY)
 			{
+				reduce_all(v, p2);
 				rp_store_global<4>(v, x, vt, T, 1);
 				continue;
 			}
-			rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1, w1q, p, q);
-			rp_radix<4, true, false>(v, vt, T, 1, LB, wi, Hr, p, q, w1, w1q);
+			rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1(vt), p, p2, pinv);
+			rp_radix<4, true>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			rp_store_smem<4>(v, sm, vt, T, 1);
 		}
 		if (J.mode == ROW_FWD_ONLY) return;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 			{
 				const u32 vt = tid + rr * NT;
 				rp_load_smem<4>(v, sm, vt, T, b);
-				rp_radix<4, true, false>(v, vt, T, b, LB, wi, Hr, p, q, w1, w1q);
+				rp_radix<4, true>(v, vt, T, b, LB, tw, Hr, p, p2);
 				rp_store_smem<4>(v, sm, vt, T, b);
 			}
 		}
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 		{
 			const u32 vt = tid + rr * NT;
 			rp_load_smem<S0>(v, sm, vt, T, B0);
-			rp_radix<S0, true, false>(v, vt, T, B0, LB, wi, Hr, p, q, w1, w1q);
+			rp_radix<S0, true>(v, vt, T, B0, LB, tw, Hr, p, p2);
 			rp_store_global<S0>(v, x, vt, T, B0);
 		}
 	}
@@ -338,11 +338,10 @@ constexpr int TW = 40;  // tile row stride: own columns + up to 8 predecessor co
 // One radix-2^S step of the column transform (levels on row bits b..b+S-1)
 // for one column of one prime: the 2^S rows that differ in those bits.
 // Global level l (2^l polynomials) works on row bit LOG_H-1-l with twiddle
-// w[2^l + j], j = row >> (LOG_H - l); level 0 of the forward direction takes
-// plain residues (rsq / w[0] trick of kernel.cl:286-290).
+// tw[2^l + j], j = row >> (LOG_H - l) (forward: w; inverse: -w^-1).
 template <int S, bool INV>
-__device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int b, u32 o, const u32 * __restrict__ tw,
-	u32 p, u32 q, u32 rsq)
+__device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int b, u32 o, const uint2 * __restrict__ tw,
+	u32 p, u32 p2)
 {
 	u32 v[1 << S];
 	const u32 row0 = (o & ((1u << b) - 1)) | ((o >> b) << (b + S));
@@ -356,31 +355,17 @@ __device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int
 	{
 		const int s = INV ? ss : (S - 1 - ss);
 		const int lvl = LOG_H - 1 - (b + s);
-		const u32 * __restrict__ twl = tw + ((1u << lvl) + (ohi << (S - 1 - s)));
+		const uint2 * __restrict__ twl = tw + ((1u << lvl) + (ohi << (S - 1 - s)));
 #pragma unroll
 		for (int jh = 0; jh < (1 << (S - 1 - s)); ++jh)
 		{
+			const uint2 wv = twl[jh];
 #pragma unroll
 			for (int gl = 0; gl < (1 << s); ++gl)
 			{
 				const int g = (jh << (s + 1)) + gl;
-				if (INV)
-				{
-					const u32 wv = twl[jh];
-					inv_bfly(v[g], v[g + (1 << s)], wv, wv * q, p);
-				}
-				else if (lvl == 0)
-				{
-					const u32 w0 = tw[0];
-					const u32 a0 = mont_mul_c(v[g], rsq, rsq * q, p), t = mont_mul_c(v[g + (1 << s)], w0, w0 * q, p);
-					v[g] = add_mod(a0, t, p);
-					v[g + (1 << s)] = sub_mod(a0, t, p);
-				}
-				else
-				{
-					const u32 wv = twl[jh];
-					fwd_bfly(v[g], v[g + (1 << s)], wv, wv * q, p);
-				}
+				if (INV) inv_bf(v[g], v[g + (1 << s)], wv.x, wv.y, p, p2);
+				else fwd_bf(v[g], v[g + (1 << s)], wv.x, wv.y, p, p2);
 			}
 		}
 	}
@@ -390,8 +375,8 @@ __device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int
 
 // All LOG_H levels of the columns u in [u0, u0 + nu) of every prime, in place
 // in the tile; stages of 3 levels (the remainder first in the forward order).
-template <int LOG_H, int K, bool INV>
-__device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const u32 * twk, const TConst & c)
+template <int LOG_H, int KP, bool INV>
+__device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const uint2 * twk, const TConst & c)
 {
 	constexpr int H = 1 << LOG_H;
 	constexpr int SR = (LOG_H % 3 == 0) ? 3 : LOG_H % 3;       // top stage (row bits LOG_H-SR..LOG_H-1)
@@ -405,193 +390,126 @@ __device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const 
 		const bool top = (idx == 0);
 		const int b = top ? (LOG_H - SR) : (LOG_H - SR - 3 * idx);
 		const int S = top ? SR : 3;
-		const int ntask = K * nu * (H >> S);
+		const int ntask = KP * nu * (H >> S);
 		for (int task = tid; task < ntask; task += NT)
 		{
 			const int u = u0 + task % nu;
 			const int rest = task / nu;
 			const int o = rest % (H >> S), k = rest / (H >> S);
 			u32 * colp = tile + (k * H) * TW + u;
-			const u32 * tw = twk + k * H;
-			if (S == 3) col_step<3, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
-			else if (S == 2) col_step<2, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
-			else col_step<1, INV>(colp, LOG_H, b, (u32)o, tw, c.p[k], c.q[k], c.rsq[k]);
+			const uint2 * tw = twk + k * H;
+			const u32 p = c.p[k];
+			if (S == 3) col_step<3, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
+			else if (S == 2) col_step<2, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
+			else col_step<1, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
 		}
 		__syncthreads();
 	}
 }
 
-// Exact value of a balanced coefficient: unsigned digits e_0 .. e_{PCK-2} and
-// the signed top digit, base 2^lb.
-template <int K, int PCK>
-__device__ __forceinline__ Big<K> digits_value(int lb, i32 top, const u32 (&e)[PCK])
+// Adds delta to the exact value of one coefficient (three limb planes, plane
+// stride PS words).
+__device__ __forceinline__ void exact_add(u32 * t, int PS, __int128 delta)
 {
-	__int128 v = (__int128)top;
-#pragma unroll
-	for (int l = PCK - 2; l >= 0; --l) v = (v << lb) + (__int128)e[l];
-	return big_from_i128<K>(v);
+	const unsigned __int128 u = (unsigned __int128)t[0] | ((unsigned __int128)t[PS] << 32) | ((unsigned __int128)t[2 * PS] << 64);
+	__int128 v = (__int128)(u << 32) >> 32;             // sign-extend the 96-bit value
+	v += delta;
+	const unsigned __int128 w = (unsigned __int128)v;
+	t[0] = (u32)w; t[PS] = (u32)(w >> 32); t[2 * PS] = (u32)(w >> 64);
 }
 
-// Second carry phase for one group of 4 coefficients, in place in the tile:
-// tp points at the group's first coefficient, plane l (digits) / k (residues)
-// at tp + l * PS.  f = carry-in; each coefficient's digits are replaced by its
-// balanced re-encoded residues (big: its exact value as K limbs); returns the
-// top sub-digit of the last coefficient (kernel.cl:1582-1613).  The loop is
-// rolled, so that the column pass body stays small enough for the
-// instruction cache; a coefficient's digits are read before its residues
-// overwrite them.
-template <int K, int PCK>
-__device__ __forceinline__ i32 carry_phase2(const TConst & c, int lb, const u32 * rbase, Big<K> f, u32 * tp, int PS, bool big, bool store)
+// Residues of the exact values of 4 coefficients (limb words l[0..2], each 4
+// coefficients) in the KP planes of the tile at tp (plane stride PS words).
+template <int KP>
+__device__ __forceinline__ void encode4(const TConst & c, const uint4 (&l)[AB_NW], u32 * tp, int PS)
 {
-	const i32 base = (i32)(1u << lb);
-	auto put = [&](int j, i32 top, const u32 (&e)[PCK]) {
-		u32 r[K];
-		if (big)
-		{
-			const Big<K> v = digits_value<K, PCK>(lb, top, e);
+	const u32 d0[4] = { l[0].x, l[0].y, l[0].z, l[0].w };
+	const u32 d1[4] = { l[1].x, l[1].y, l[1].z, l[1].w };
+	const u32 d2[4] = { l[2].x ^ 0x80000000u, l[2].y ^ 0x80000000u, l[2].z ^ 0x80000000u, l[2].w ^ 0x80000000u };
 #pragma unroll
-			for (int k = 0; k < K; ++k) r[k] = v.l[k];
-		}
-		else encode_digits<K, PCK>(c, rbase, top, e, r);
-		if (store)
-		{
-#pragma unroll
-			for (int k = 0; k < K; ++k) tp[k * PS + j] = r[k];
-		}
-	};
-#pragma unroll 1
-	for (int j = 0; j < 3; ++j)
+	for (int k = 0; k < KP; ++k)
 	{
-		u32 d[PCK];
-#pragma unroll
-		for (int l = 0; l < PCK; ++l) d[l] = tp[l * PS + j];
-		f = add_digits<K, PCK>(f, lb, d);
-		u32 e[PCK];
-		extract_shift<K, PCK>(f, lb, e);
-		i32 top = (i32)e[PCK - 1];
-		if (top >= base / 2) { top -= base; f = big_add_u32<K>(f, 1u); }
-		put(j, top, e);
+		uint4 r;
+		r.x = encode_res(c, k, d0[0], d1[0], d2[0]);
+		r.y = encode_res(c, k, d0[1], d1[1], d2[1]);
+		r.z = encode_res(c, k, d0[2], d1[2], d2[2]);
+		r.w = encode_res(c, k, d0[3], d1[3], d2[3]);
+		*reinterpret_cast<uint4 *>(tp + k * PS) = r;
 	}
-	{
-		u32 d[PCK];
-#pragma unroll
-		for (int l = 0; l < PCK; ++l) d[l] = tp[l * PS + 3];
-		f = add_digits<K, PCK>(f, lb, d);
-	}
-	const u32 bm = (u32)base - 1;
-	u32 e[PCK];
-	i32 top;
-	if (PCK == 1)
-	{
-		top = (i32)(i64)big_low64<K>(f);
-	}
-	else if (PCK == 2)
-	{
-		const i64 r01 = (i64)big_low64<K>(f);
-		e[0] = (u32)r01 & bm;
-		top = (i32)(r01 >> lb);
-	}
-	else
-	{
-		const u64 r01 = big_low64<K>(f) & (((u64)1 << (2 * lb)) - 1);
-		e[0] = (u32)r01 & bm;
-		e[1 % PCK] = (u32)(r01 >> lb);
-		const Big<K> f23 = big_sar<K>(f, 2 * lb);
-		const i64 r23 = (i64)big_low64<K>(f23);
-		e[2 % PCK] = (u32)r23 & bm;
-		top = (i32)(r23 >> lb);
-	}
-	put(3, top, e);
-	return top;
 }
 
-// The same second phase unrolled over the 4 coefficients (faster for tall
-// columns, LOG_H >= 5, where the body fits the instruction cache less badly
-// than the lost parallelism costs): f = carry-in, d = the group's unsigned digits; writes the balanced re-encoded residues (BIG: the
-// exact coefficient values as K limbs) and returns the top sub-digit of the
-// last coefficient (kernel.cl:1582-1613).
-template <int K, int PCK, bool BIG>
-__device__ __forceinline__ i32 carry_phase2_unrolled(const TConst & c, int lb, const u32 * rbase, Big<K> f, const u32 (&d)[4][PCK], u32 (&res)[4][K])
+// Second carry phase for one group of 4 coefficients (kernel.cl:1582-1613):
+// f = carry-in, d = the group's unsigned digits; returns each coefficient's
+// exact value (balanced top digit, the last coefficient absorbing the rest)
+// as three limbs and the top sub-digit of the last coefficient.
+template <int L, int PCK>
+__device__ __forceinline__ i32 carry_phase2(int lb, Big<L> f, const u32 (&d)[4][PCK], u32 (&x)[AB_NW][4])
 {
 	const i32 base = (i32)(1u << lb);
 #pragma unroll
 	for (int j = 0; j < 3; ++j)
 	{
-		f = add_digits<K, PCK>(f, lb, d[j]);
+		f = add_digits<L, PCK>(f, lb, d[j]);
 		u32 e[PCK];
-		extract_shift<K, PCK>(f, lb, e);
+		extract_shift<L, PCK>(f, lb, e);
 		i32 top = (i32)e[PCK - 1];
-		if (top >= base / 2) { top -= base; f = big_add_u32<K>(f, 1u); }
-		if (BIG)
-		{
-			const Big<K> v = digits_value<K, PCK>(lb, top, e);
-#pragma unroll
-			for (int k = 0; k < K; ++k) res[j][k] = v.l[k];
-		}
-		else encode_digits<K, PCK>(c, rbase, top, e, res[j]);
+		if (top >= base / 2) { top -= base; f = big_add_u32<L>(f, 1u); }
+		digits_exact<PCK>(lb, top, e, x[0][j], x[1][j], x[2][j]);
 	}
-	f = add_digits<K, PCK>(f, lb, d[3]);
+	f = add_digits<L, PCK>(f, lb, d[3]);
 	const u32 bm = (u32)base - 1;
 	u32 e[PCK];
 	i32 top;
 	if (PCK == 1)
 	{
-		top = (i32)(i64)big_low64<K>(f);
+		top = (i32)(i64)big_low64<L>(f);
 	}
 	else if (PCK == 2)
 	{
-		const i64 r01 = (i64)big_low64<K>(f);
+		const i64 r01 = (i64)big_low64<L>(f);
 		e[0] = (u32)r01 & bm;
 		top = (i32)(r01 >> lb);
 	}
 	else
 	{
-		const u64 r01 = big_low64<K>(f) & (((u64)1 << (2 * lb)) - 1);
+		const u64 r01 = big_low64<L>(f) & (((u64)1 << (2 * lb)) - 1);
 		e[0] = (u32)r01 & bm;
 		e[1 % PCK] = (u32)(r01 >> lb);
-		const Big<K> f23 = big_sar<K>(f, 2 * lb);
-		const i64 r23 = (i64)big_low64<K>(f23);
+		const Big<L> f23 = big_sar<L>(f, 2 * lb);
+		const i64 r23 = (i64)big_low64<L>(f23);
 		e[2 % PCK] = (u32)r23 & bm;
 		top = (i32)(r23 >> lb);
 	}
-	if (BIG)
-	{
-		const Big<K> v = digits_value<K, PCK>(lb, top, e);
-#pragma unroll
-		for (int k = 0; k < K; ++k) res[3][k] = v.l[k];
-	}
-	else encode_digits<K, PCK>(c, rbase, top, e, res[3]);
+	digits_exact<PCK>(lb, top, e, x[0][3], x[1][3], x[2][3]);
 	return top;
 }
 
 template <int LOG_H, int K, int PCK>
 __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, const TConst c)
 {
+	constexpr int KP = K + 1, L = K;             // transform primes, limbs of the carry
 	constexpr int H = 1 << LOG_H;
-	// carry loops rolled over the 4 coefficients of a group for short columns,
-	// unrolled for tall ones (measured: 12 % faster at LOG_H = 3 with K = 5,
-	// equal at 4, 2 % slower at 5 and 6)
-	constexpr bool ROLL = (LOG_H <= 4);
+	constexpr int PS = H * TW;                   // tile plane stride
 	extern __shared__ __align__(16) u32 sm[];
-	u32 * const tile = sm;                       // [K][H][TW]
-	u32 * const cw = tile + K * H * TW;          // [H][TW/4][K] carry-out words
-	u32 * const twc = cw + H * (TW / 4) * K;     // [3][K][H] column twiddles
+	u32 * const tile = sm;                       // [KP][H][TW]
+	u32 * const cw = tile + KP * PS;             // [H][TW/4][L] carry-out words
+	uint2 * const twc = reinterpret_cast<uint2 *>(cw + H * (TW / 4) * L);   // [3][KP][H] column twiddles
 	__shared__ int decision;
-	__shared__ CandConst cc;
 
 	ColJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
 	const u32 cand = blockIdx.z;
 	const u32 amul = (J.mult != nullptr) ? J.mult[cand] : J.a;
 	if (amul == 0u) return;                       // inactive batch slot
 	{
-		const size_t cofs = (size_t)cand * J.stride;
-		J.in += cofs;
-		if (J.sub) J.sub += cofs;
-		if (J.out_norm) J.out_norm += cofs;
-		if (J.out_fwd[0]) J.out_fwd[0] += cofs;
-		if (J.out_fwd[1]) J.out_fwd[1] += cofs;
-		if (J.out_snap) J.out_snap = (J.snap_flag[cand] != 0u) ? J.out_snap + cofs : nullptr;
+		const size_t on = (size_t)cand * J.stride_norm, ot = (size_t)cand * J.stride_ntt;
+		J.in += J.transformed ? ot : on;
+		if (J.sub) J.sub += on;
+		if (J.out_norm) J.out_norm += on;
+		if (J.out_fwd[0]) J.out_fwd[0] += ot;
+		if (J.out_fwd[1]) J.out_fwd[1] += ot;
+		if (J.out_snap) J.out_snap = (J.snap_flag[cand] != 0u) ? J.out_snap + on : nullptr;
 	}
+	const int lb = (J.cand != nullptr) ? J.cand[cand].lbase : c.lbase;
 	const u32 R = c.R, n = c.n;
 	const int nb = (int)gridDim.x, b = (int)blockIdx.x;
 	const u32 c0 = (u32)b * CC;
@@ -602,138 +520,87 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	const int E = (!J.transformed || single) ? 0 : ((b == 0 && J.lower != LOWER_NONE) ? 8 : 4);
 	const int WU = CC + E, ng = WU / 4;
 	const int tid = (int)threadIdx.x, NT = (int)blockDim.x;
-	if (tid == 0)
-	{
-		if (J.cand != nullptr) cc = J.cand[cand];
-		else
-		{
-			cc.lbase = c.lbase;
-			for (int k = 0; k < AB_MAXK; ++k) { cc.rbase[k] = c.rbase[k]; cc.rbase_pck[k] = c.rbase_pck[k]; }
-		}
-	}
 
 	auto gcol = [&](int u) -> u32 { return (u < E) ? ((b == 0) ? R - (u32)E + (u32)u : c0 - (u32)E + (u32)u) : c0 + (u32)(u - E); };
 
-	// ---- load the tile and the column twiddles
-	for (int idx = tid; idx < K * H * ng; idx += NT)
+	// ---- load the tile (NTT form: KP planes; normal form: the three limb
+	// planes) and the column twiddles
+	const int np_in = J.transformed ? KP : AB_NW;
+	for (int idx = tid; idx < np_in * H * ng; idx += NT)
 	{
 		const int u4 = idx % ng, row = (idx / ng) % H, k = idx / (ng * H);
 		const uint4 val = __ldg(reinterpret_cast<const uint4 *>(J.in + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
-		*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + 4 * u4) = val;
+		*reinterpret_cast<uint4 *>(tile + k * PS + row * TW + 4 * u4) = val;
 	}
-	for (int idx = tid; idx < K * H; idx += NT)
+	const size_t hn = n >> 1;                    // twiddle pairs per prime
+	for (int idx = tid; idx < KP * H; idx += NT)
 	{
 		const int k = idx / H, i = idx % H;
-		if (J.transformed) twc[idx] = J.w_in[(size_t)k * n + (n >> 1) + i];
-		if (J.out_fwd[0] != nullptr) twc[K * H + idx] = J.w_out[0][(size_t)k * n + i];
-		if (J.out_fwd[1] != nullptr) twc[2 * K * H + idx] = J.w_out[1][(size_t)k * n + i];
+		if (i == 0) continue;
+		if (J.transformed)
+		{
+			// -w^-1 of the source domain: its own table (R) or the mirror of w (Q)
+			const int s = 1 << (31 - __clz(i));
+			twc[idx] = (J.wi_in != nullptr) ? J.wi_in[(size_t)k * hn + i] : J.w_in[(size_t)k * hn + (3 * s - 1 - i)];
+		}
+		if (J.out_fwd[0] != nullptr) twc[KP * H + idx] = J.w_out[0][(size_t)k * hn + i];
+		if (J.out_fwd[1] != nullptr) twc[2 * KP * H + idx] = J.w_out[1][(size_t)k * hn + i];
 	}
 	if (tid == 0) decision = 0;
 	__syncthreads();
-	const int lb = cc.lbase;
 
 	if (J.transformed)
 	{
-		// ---- inverse column levels (all WU columns, K primes)
-		col_transform<LOG_H, K, true>(tile, 0, WU, twc, c);
+		// ---- inverse column levels (all WU columns, KP primes)
+		col_transform<LOG_H, KP, true>(tile, 0, WU, twc, c);
 
-		// ---- carry phase 1: per group, unsigned digits + carry-out
+		// ---- carry phase 1: per group, exact values (CRT), x a, - sub,
+		// unsigned digits + carry-out
 		for (int idx = tid; idx < H * ng; idx += NT)
 		{
 			const int row = idx / ng, u4 = idx % ng;
 			if (E == 8 && u4 == 0 && row != H - 1) continue;
-			Big<K> f;
-			if constexpr (ROLL)
+			u32 xv[KP][4];
+#pragma unroll
+			for (int k = 0; k < KP; ++k)
 			{
-				// rolled over the 4 coefficients (code size); coefficient j's digits
-				// overwrite its residues once they are read
-				u32 * const tp = tile + row * TW + 4 * u4;
-				const u32 * const sp = (J.sub != nullptr) ? J.sub + (size_t)row * R + gcol(4 * u4) : nullptr;
-				f = big_zero<K>();
-#pragma unroll 1
-				for (int j = 0; j < 4; ++j)
+				const uint4 t = *reinterpret_cast<const uint4 *>(tile + k * PS + row * TW + 4 * u4);
+				xv[k][0] = t.x; xv[k][1] = t.y; xv[k][2] = t.z; xv[k][3] = t.w;
+			}
+			u32 sv[AB_NW][4];
+			if (J.sub != nullptr)
+			{
+#pragma unroll
+				for (int l = 0; l < AB_NW; ++l)
 				{
-					u32 rr[K];
-#pragma unroll
-					for (int k = 0; k < K; ++k) rr[k] = mont_mul(tp[k * H * TW + j], c.norm[k], c.p[k], c.q[k]);
-					const Big<K> V = garner<K>(c, rr);
-					f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
-					if (sp != nullptr)
-					{
-#pragma unroll
-						for (int k = 0; k < K; ++k) rr[k] = __ldg(sp + (size_t)k * n + j);
-						Big<K> sv;
-						if (J.sub_big)
-						{
-#pragma unroll
-							for (int k = 0; k < K; ++k) sv.l[k] = rr[k];
-						}
-						else sv = garner<K>(c, rr);
-						f = big_sub<K>(f, sv);
-					}
-					u32 dg[PCK];
-					extract_shift<K, PCK>(f, lb, dg);
-#pragma unroll
-					for (int l = 0; l < PCK; ++l) tp[l * H * TW + j] = dg[l];
+					const uint4 t = __ldg(reinterpret_cast<const uint4 *>(J.sub + (size_t)l * n + (size_t)row * R + gcol(4 * u4)));
+					sv[l][0] = t.x; sv[l][1] = t.y; sv[l][2] = t.z; sv[l][3] = t.w;
 				}
 			}
-			else
+			Big<L> f = big_zero<L>();
+			u32 dg[4][PCK];
+#pragma unroll
+			for (int j = 0; j < 4; ++j)
 			{
-				u32 xv[K][4];
+				u32 rr[KP];
 #pragma unroll
-				for (int k = 0; k < K; ++k)
-				{
-					const uint4 t = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + 4 * u4);
-					xv[k][0] = t.x; xv[k][1] = t.y; xv[k][2] = t.z; xv[k][3] = t.w;
-				}
-				u32 sv[K][4];
-				if (J.sub != nullptr)
-				{
-#pragma unroll
-					for (int k = 0; k < K; ++k)
-					{
-						const uint4 t = __ldg(reinterpret_cast<const uint4 *>(J.sub + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
-						sv[k][0] = t.x; sv[k][1] = t.y; sv[k][2] = t.z; sv[k][3] = t.w;
-					}
-				}
-				f = big_zero<K>();
-				u32 dg[4][PCK];
-#pragma unroll
-				for (int j = 0; j < 4; ++j)
-				{
-					u32 rr[K];
-#pragma unroll
-					for (int k = 0; k < K; ++k) rr[k] = mont_mul(xv[k][j], c.norm[k], c.p[k], c.q[k]);
-					const Big<K> V = garner<K>(c, rr);
-					f = big_add<K>(f, (amul == 1u) ? V : big_mul_u32<K>(V, amul));
-					if (J.sub != nullptr)
-					{
-						Big<K> s;
-						if (J.sub_big)
-						{
-#pragma unroll
-							for (int k = 0; k < K; ++k) s.l[k] = sv[k][j];
-						}
-						else
-						{
-#pragma unroll
-							for (int k = 0; k < K; ++k) rr[k] = sv[k][j];
-							s = garner<K>(c, rr);
-						}
-						f = big_sub<K>(f, s);
-					}
-					extract_shift<K, PCK>(f, lb, dg[j]);
-				}
-#pragma unroll
-				for (int l = 0; l < PCK; ++l)
-					*reinterpret_cast<uint4 *>(tile + (l * H + row) * TW + 4 * u4) = make_uint4(dg[0][l], dg[1][l], dg[2][l], dg[3][l]);
+				for (int k = 0; k < KP; ++k) rr[k] = xv[k][j];
+				Big<L> V = crt<L>(c, rr);
+				if (amul != 1u) V = big_mul_u32<L>(V, amul);
+				if (J.sub != nullptr) V = big_sub<L>(V, big_from_exact<L>(sv[0][j], sv[1][j], sv[2][j]));
+				f = big_add<L>(f, V);
+				extract_shift<L, PCK>(f, lb, dg[j]);
 			}
 #pragma unroll
-			for (int k = 0; k < K; ++k) cw[(row * (TW / 4) + u4) * K + k] = f.l[k];
+			for (int l = 0; l < PCK; ++l)
+				*reinterpret_cast<uint4 *>(tile + l * PS + row * TW + 4 * u4) = make_uint4(dg[0][l], dg[1][l], dg[2][l], dg[3][l]);
+#pragma unroll
+			for (int l = 0; l < L; ++l) cw[(row * (TW / 4) + u4) * L + l] = f.l[l];
 		}
 		__syncthreads();
 
-		// ---- carry phase 2: add the previous group's carry-out, balanced re-encode
+		// ---- carry phase 2: add the previous group's carry-out, balanced
+		// digits, exact values
 		const int own_groups = CC / 4;
 		for (int idx = tid; idx < H * own_groups + 1; idx += NT)
 		{
@@ -759,31 +626,24 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 				if (row > 0) prow = row - 1;
 				else { prow = H - 1; neg = (J.nega != 0); }
 			}
-			Big<K> f;
+			Big<L> f;
 #pragma unroll
-			for (int k = 0; k < K; ++k) f.l[k] = cw[(prow * (TW / 4) + pu4) * K + k];
-			if (neg) f = big_neg<K>(f);
-			i32 top;
-			if constexpr (ROLL)
-				top = carry_phase2<K, PCK>(c, lb, cc.rbase, f, tile + row * TW + 4 * u4, H * TW, J.out_big != 0, store);
-			else
+			for (int l = 0; l < L; ++l) f.l[l] = cw[(prow * (TW / 4) + pu4) * L + l];
+			if (neg) f = big_neg<L>(f);
+			u32 dg[4][PCK];
+#pragma unroll
+			for (int l = 0; l < PCK; ++l)
 			{
-				u32 dg[4][PCK];
+				const uint4 t = *reinterpret_cast<const uint4 *>(tile + l * PS + row * TW + 4 * u4);
+				dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
+			}
+			u32 ex[AB_NW][4];
+			const i32 top = carry_phase2<L, PCK>(lb, f, dg, ex);
+			if (store)
+			{
 #pragma unroll
-				for (int l = 0; l < PCK; ++l)
-				{
-					const uint4 t = *reinterpret_cast<const uint4 *>(tile + (l * H + row) * TW + 4 * u4);
-					dg[0][l] = t.x; dg[1][l] = t.y; dg[2][l] = t.z; dg[3][l] = t.w;
-				}
-				u32 res[4][K];
-				top = J.out_big ? carry_phase2_unrolled<K, PCK, true>(c, lb, cc.rbase, f, dg, res)
-				                : carry_phase2_unrolled<K, PCK, false>(c, lb, cc.rbase, f, dg, res);
-				if (store)
-				{
-#pragma unroll
-					for (int k = 0; k < K; ++k)
-						*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + 4 * u4) = make_uint4(res[0][k], res[1][k], res[2][k], res[3][k]);
-				}
+				for (int l = 0; l < AB_NW; ++l)
+					*reinterpret_cast<uint4 *>(tile + l * PS + row * TW + 4 * u4) = make_uint4(ex[l][0], ex[l][1], ex[l][2], ex[l][3]);
 			}
 			const bool is_last = (row == H - 1) && (u4 == ng - 1) && (b == nb - 1);
 			if ((is_last || !store) && top >= (i32)(1u << lb)) decision = 1;
@@ -791,74 +651,140 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 		__syncthreads();
 
 		// ---- mod R (+2) / mod Q on the top and bottom coefficients (kernel.cl:1653-1683)
-		if (J.lower != LOWER_NONE && tid < K)
+		if (J.lower != LOWER_NONE && tid == 0)
 		{
-			const int k = tid;
-			const u32 p = c.p[k];
-			if (decision)
+			if (decision && b == nb - 1) exact_add(tile + (H - 1) * TW + WU - 1, PS, -((__int128)1 << (c.pck * lb)));
+			if (b == 0)
 			{
-				if (b == nb - 1)
-				{
-					u32 & t = tile[(k * H + H - 1) * TW + WU - 1];
-					t = sub_mod(t, cc.rbase_pck[k], p);
-				}
-				if (b == 0)
-				{
-					u32 & t = tile[(k * H) * TW + E];
-					t = sub_mod(t, set_i32((J.lower == LOWER_Q) ? 1 : -1, p), p);
-				}
-			}
-			if (J.lower == LOWER_R_ADD2 && b == 0)
-			{
-				u32 & t = tile[(k * H) * TW + E];
-				t = add_mod(t, 2u, p);
+				int d = 0;
+				if (decision) d += (J.lower == LOWER_Q) ? -1 : 1;
+				if (J.lower == LOWER_R_ADD2) d += 2;
+				if (d != 0) exact_add(tile + E, PS, (__int128)d);
 			}
 		}
 		__syncthreads();
 	}
 
 	// ---- outputs: normal form, then the first LA forward levels of the next
-	// product, computed in place (the second domain reloads the normal form
-	// from global memory)
+	// product in one or two domains (the residues are encoded from the exact
+	// values in the tile, or for the second domain from the normal form in
+	// global memory)
 	if (J.out_norm != nullptr || J.out_snap != nullptr)
 	{
-		for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
+		for (int idx = tid; idx < AB_NW * H * (CC / 4); idx += NT)
 		{
-			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
-			const uint4 val = *reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + E + 4 * u4);
-			const size_t o = (size_t)k * n + (size_t)row * R + c0 + 4 * u4;
+			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, l = idx / ((CC / 4) * H);
+			const uint4 val = *reinterpret_cast<const uint4 *>(tile + l * PS + row * TW + E + 4 * u4);
+			const size_t o = (size_t)l * n + (size_t)row * R + c0 + 4 * u4;
 			if (J.out_norm) *reinterpret_cast<uint4 *>(J.out_norm + o) = val;
 			if (J.out_snap) *reinterpret_cast<uint4 *>(J.out_snap + o) = val;
 		}
-		__syncthreads();
 	}
-	bool reload = false;
+	bool first = true;
 #pragma unroll 1
 	for (int dom = 0; dom < 2; ++dom)
 	{
 		u32 * const out = (dom == 0) ? J.out_fwd[0] : J.out_fwd[1];
 		if (out == nullptr) continue;
-		if (reload)
+		__syncthreads();
+		const u32 * src = first ? nullptr : (J.transformed ? J.out_norm : J.in);
+		for (int idx = tid; idx < H * (CC / 4); idx += NT)
 		{
-			__syncthreads();
-			const u32 * src = J.transformed ? J.out_norm : J.in;
-			for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
-			{
-				const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
-				*reinterpret_cast<uint4 *>(tile + (k * H + row) * TW + E + 4 * u4) =
-					*reinterpret_cast<const uint4 *>(src + (size_t)k * n + (size_t)row * R + c0 + 4 * u4);
-			}
-			__syncthreads();
+			const int u4 = idx % (CC / 4), row = idx / (CC / 4);
+			u32 * const tp = tile + row * TW + E + 4 * u4;
+			uint4 l[AB_NW];
+#pragma unroll
+			for (int i = 0; i < AB_NW; ++i)
+				l[i] = (src == nullptr) ? *reinterpret_cast<const uint4 *>(tp + i * PS)
+				                        : *reinterpret_cast<const uint4 *>(src + (size_t)i * n + (size_t)row * R + c0 + 4 * u4);
+			encode4<KP>(c, l, tp, PS);
 		}
-		col_transform<LOG_H, K, false>(tile, E, CC, twc + (1 + dom) * K * H, c);
-		for (int idx = tid; idx < K * H * (CC / 4); idx += NT)
+		__syncthreads();
+		col_transform<LOG_H, KP, false>(tile, E, CC, twc + (1 + dom) * KP * H, c);
+		for (int idx = tid; idx < KP * H * (CC / 4); idx += NT)
 		{
 			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
 			*reinterpret_cast<uint4 *>(out + (size_t)k * n + (size_t)row * R + c0 + 4 * u4) =
-				*reinterpret_cast<const uint4 *>(tile + (k * H + row) * TW + E + 4 * u4);
+				*reinterpret_cast<const uint4 *>(tile + k * PS + row * TW + E + 4 * u4);
 		}
-		reload = true;
+		first = false;
 	}
+}
+
+// ================================================================ register words of the reference
+// Canonical residue of the exact value (d0, d1, d2) mod a reference prime:
+// d0 + d1 2^32 + d2 2^64 with Montgomery steps (r2 = 2^64 mod p, so
+// ref_mont(x, r2) = x 2^32 mod p); a negative value is negated first.
+__device__ __forceinline__ u32 ref_mont(u32 a, u32 b, u32 p, u32 q)
+{
+	const u64 t = (u64)a * b;
+	const u32 m = (u32)t * q;
+	return ref_sub((u32)(t >> 32), __umulhi(m, p), p);
+}
+
+__device__ __forceinline__ u32 ref_add(u32 a, u32 b, u32 p) { return ref_sub(a, p - b, p); }
+
+__global__ void k_export(const RefConst rc, const u32 * __restrict__ norm, u32 * __restrict__ words, u32 n)
+{
+	const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	u32 d0 = norm[i], d1 = norm[n + i], d2 = norm[2 * (size_t)n + i];
+	const bool neg = (i32)d2 < 0;
+	if (neg)
+	{
+		// two's-complement negation of the 96-bit value
+		d0 = ~d0; d1 = ~d1; d2 = ~d2;
+		d0 += 1; if (d0 == 0) { d1 += 1; if (d1 == 0) d2 += 1; }
+	}
+	for (int k = 0; k < rc.K; ++k)
+	{
+		const u32 p = rc.p[k], q = rc.q[k], r2 = rc.r2[k];
+		const u32 a0 = ref_red(d0, p);
+		const u32 a1 = ref_mont(d1, r2, p, q);                       // d1 2^32
+		const u32 a2 = ref_mont(ref_mont(d2, r2, p, q), r2, p, q);   // d2 2^64
+		u32 r = ref_add(ref_add(a0, a1, p), a2, p);
+		if (neg && r != 0) r = p - r;
+		words[(size_t)k * n + i] = r;
+	}
+}
+
+// Exact signed value from the K residues (mixed-radix Garner, leading digit
+// balanced; kernel.cl:1231-1470), checked against the 96-bit normal form.
+template <int K>
+__global__ void k_import(const RefConst rc, const u32 * __restrict__ words, u32 * __restrict__ norm, u32 n, u32 * bad)
+{
+	const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	u32 u[K];
+#pragma unroll
+	for (int ii = K - 1; ii >= 0; --ii)
+	{
+		u32 v = words[(size_t)ii * n + i];
+#pragma unroll
+		for (int j = K - 1; j > ii; --j) v = ref_mont_c(ref_sub(v, u[j], rc.p[ii]), rc.gm[ii][j], rc.gmq[ii][j], rc.p[ii]);
+		u[ii] = v;
+	}
+	const i32 i0 = (u[0] > (rc.p[0] >> 1)) ? (i32)(u[0] - rc.p[0]) : (i32)u[0];
+	Big<K> V;
+	{
+		const i64 v01 = (i64)i0 * (i64)rc.p[1] + (i64)u[1];
+		V.l[0] = (u32)v01; V.l[1] = (u32)((u64)v01 >> 32);
+		const u32 sgn = (v01 < 0) ? 0xffffffffu : 0u;
+#pragma unroll
+		for (int l = 2; l < K; ++l) V.l[l] = sgn;
+	}
+#pragma unroll
+	for (int l = 2; l < K; ++l) V = big_add_u32<K>(big_mul_u32<K>(V, rc.p[l]), u[l]);
+	const u32 sgn = big_is_neg<K>(V) ? 0xffffffffu : 0u;
+	u32 x[AB_NW];
+#pragma unroll
+	for (int l = 0; l < AB_NW; ++l) x[l] = (l < K) ? V.l[l] : sgn;
+	bool fits = (K < AB_NW) || (((i32)x[2] < 0) == (sgn != 0));
+#pragma unroll
+	for (int l = AB_NW; l < K; ++l) fits = fits && (V.l[l] == sgn);
+	if (!fits) atomicOr(bad, 1u);
+#pragma unroll
+	for (int l = 0; l < AB_NW; ++l) norm[(size_t)l * n + i] = x[l];
 }
 
 // ================================================================ host side
@@ -878,9 +804,10 @@ bool make_geometry(int ln, int lb_override, Geometry & g)
 	return true;
 }
 
-size_t colpass_smem(const Geometry & g, int K)
+size_t colpass_smem(const Geometry & g, int KP)
 {
-	return sizeof(u32) * ((size_t)K * g.H * TW + (size_t)g.H * (TW / 4) * K + 3 * (size_t)K * g.H);
+	const size_t L = (size_t)KP - 1;
+	return sizeof(u32) * ((size_t)KP * g.H * TW + (size_t)g.H * (TW / 4) * L) + sizeof(uint2) * 3 * (size_t)KP * g.H;
 }
 
 // The dynamic shared-memory limit of a kernel is a per-device setting: set it
@@ -907,7 +834,7 @@ static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs
 	const cudaError_t e = allow_dynamic_smem(k_rowpass<LOG_R>, smem, attr_done);
 	if (e != cudaSuccess) return e;
 	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
-	const dim3 grid((unsigned)(c.K * g.H), (unsigned)njobs, (unsigned)ncand);
+	const dim3 grid((unsigned)(c.KP * g.H), (unsigned)njobs, (unsigned)ncand);
 	k_rowpass<LOG_R><<<grid, RowCfg<LOG_R>::NT, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
@@ -933,7 +860,7 @@ cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs &
 template <int LOG_H, int K, int PCK>
 static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
-	const size_t smem = colpass_smem(g, K);
+	const size_t smem = colpass_smem(g, K + 1);
 	static std::atomic<unsigned long long> attr_done{0};
 	const cudaError_t e = allow_dynamic_smem(k_colpass<LOG_H, K, PCK>, smem, attr_done);
 	if (e != cudaSuccess) return e;
@@ -968,6 +895,28 @@ cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs &
 	case 5: return colpass_k<5, 4>(g, c, jobs, njobs, s, ncand);
 	default: return cudaErrorInvalidValue;
 	}
+}
+
+cudaError_t launch_export(const RefConst & rc, const u32 * norm, u32 * words, u32 n, cudaStream_t s)
+{
+	if (n == 0) return cudaSuccess;
+	k_export<<<(n + 255) / 256, 256, 0, s>>>(rc, norm, words, n);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_import(const RefConst & rc, const u32 * words, u32 * norm, u32 n, u32 * bad, cudaStream_t s)
+{
+	if (n == 0) return cudaSuccess;
+	const unsigned nb = (n + 255) / 256;
+	switch (rc.K)
+	{
+	case 2: k_import<2><<<nb, 256, 0, s>>>(rc, words, norm, n, bad); break;
+	case 3: k_import<3><<<nb, 256, 0, s>>>(rc, words, norm, n, bad); break;
+	case 4: k_import<4><<<nb, 256, 0, s>>>(rc, words, norm, n, bad); break;
+	case 5: k_import<5><<<nb, 256, 0, s>>>(rc, words, norm, n, bad); break;
+	default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
 }
 
 } // namespace ab

@@ -1,14 +1,23 @@
 // Launch interface of the NTT passes (host side).
 //
-// Transform layout: one register = K planes of n = 2^ln residues (plane k at
-// offset k*n).  The length-n negacyclic/cyclic NTT of the reference
-// (ocl/kernel.cl: LN-1 radix-2 levels, then a pointwise product of degree-1
-// polynomials) is split 2-D: coefficient i = row*R + col, H rows, R columns.
-//   * column pass (k_colpass): the first LA = log2(H) levels (strides >= R),
-//     fused with the inverse of those levels, the carry of the previous product
-//     and the first levels of the next product;
-//   * row pass (k_rowpass): the last LB levels (strides < R), the pointwise
-//     square / multiply, and the inverse of those LB levels, one CTA per row.
+// Layouts (all words u32):
+// * NTT form: KP planes of n = 2^ln lazy residues mod the transform primes
+//   (plane k at offset k*n).  The length-n cyclic (domain R, x^n - 1) or
+//   negacyclic (domain Q, x^n + 1) transform is ln - 1 radix-2 levels that
+//   split the register into n/2 polynomials of degree 1 (ocl/kernel.cl), split
+//   2-D: coefficient i = row*R + col, H rows, R columns.
+//     * column pass (k_colpass): the first LA = log2(H) levels (strides >= R),
+//       fused with the inverse of those levels, the carry of the previous
+//       product and the first levels of the next product;
+//     * row pass (k_rowpass): the last LB levels (strides < R), the pointwise
+//       square / multiply, and the inverse of those LB levels, one CTA per row.
+// * Normal form: AB_NW = 3 planes of n words, the limbs (low first) of each
+//   coefficient's exact value in two's complement.
+// * Twiddles of one domain and prime: forward table w of n/2 Shoup pairs
+//   (w, floor(w 2^32/p)) at the reference's bit-reversed positions (level
+//   with s polynomials: index s + bitrev(j, s), s = n/4 .. 1); domain R also
+//   has a table of -w^-1 at the same positions.  Domain Q needs none: there
+//   -w_j^-1 = w_{s-1-j}, the forward twiddle at the mirrored position.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -24,11 +33,12 @@ enum RowMode { ROW_FWD_ONLY = 0, ROW_SQUARE = 1, ROW_MUL = 2 };
 // candidate, 0 = skip it.
 struct RowJob
 {
-	u32 * x;          // K x n buffer, rows transformed in place
-	const u32 * xp;   // ROW_MUL: pre-transformed operand (same layout)
-	const u32 * w;    // twiddles of the domain: per prime n words, w (n/2) || wi (n/2)
+	u32 * x;          // KP x n buffer, rows transformed in place
+	const u32 * xp;   // ROW_MUL: full forward image of the other operand (same layout)
+	const uint2 * w;  // forward twiddles of the domain: per prime n/2 pairs
+	const uint2 * wi; // domain R: -w^-1 table (n/2 pairs per prime); null = domain Q (mirrored w)
 	int mode;
-	size_t stride;
+	size_t stride;    // words between candidates (x and xp)
 	const u32 * active;
 };
 struct RowJobs { RowJob j[2]; };
@@ -38,21 +48,20 @@ enum LowerMode { LOWER_NONE = 0, LOWER_R_ADD2 = 1, LOWER_Q = 2 };
 struct ColJob
 {
 	const u32 * in;      // source buffer
-	int transformed;     // 1: source awaits the inverse column levels + carry; 0: normal-form residues
-	const u32 * w_in;    // twiddles of the source domain (transformed source)
+	int transformed;     // 1: NTT-form source awaiting the inverse column levels + carry; 0: normal form
+	const uint2 * w_in;  // forward twiddles of the source domain (transformed source)
+	const uint2 * wi_in; // its -w^-1 table (domain R) or null (domain Q)
 	u32 a;               // carry: multiply by a
 	int nega;            // carry: wrap-around negated (mod x^n + 1)
 	const u32 * sub;     // carry: subtract this normal-form register (nullable)
-	int sub_big;         // 1: `sub` holds exact coefficient values (K two's-complement limbs per coefficient, as out_big writes)
 	int lower;           // LowerMode applied after the carry
 	u32 * out_norm;      // normal-form result (nullable)
-	int out_big;         // 1: out_norm receives each coefficient's exact value (K limbs, plane k = limb k)
-	                     // instead of its residues -- for T_Q, which only the subtracting carry reads
 	u32 * out_fwd[2];    // first LA forward levels of the result, per domain (nullable)
-	const u32 * w_out[2];
-	size_t stride;       // words between candidates (batches)
+	const uint2 * w_out[2];
+	size_t stride_ntt;   // words between candidates of NTT-form buffers (in when transformed, out_fwd)
+	size_t stride_norm;  // words between candidates of normal-form buffers (in when not, sub, out_norm, out_snap)
 	const u32 * mult;    // per candidate: the carry multiplier a, 0 = inactive (nullable: use `a`)
-	const CandConst * cand;  // per-candidate digit constants (nullable: those of TConst)
+	const CandConst * cand;  // per-candidate digit size (nullable: that of TConst)
 	u32 * out_snap;      // per candidate: also store the normal form here when snap_flag[z] != 0
 	const u32 * snap_flag;
 };
@@ -65,13 +74,20 @@ struct Geometry
 	int C;               // columns per column-pass CTA
 };
 
-// Chooses the 2-D split for a transform of length 2^ln (6 <= ln <= 21).
+// Chooses the 2-D split for a transform of length 2^ln (6 <= ln <= 20).
 bool make_geometry(int ln, int lb_override, Geometry & g);
 
 // Column-pass scratch in shared memory, bytes.
-size_t colpass_smem(const Geometry & g, int K);
+size_t colpass_smem(const Geometry & g, int KP);
 
 cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
 cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
+
+// Register words of the reference (K planes of residues mod its primes) from
+// the normal form, and back.  The import sets *bad when a coefficient's value
+// does not fit the 96-bit normal form (the words are not a normal-form
+// register).
+cudaError_t launch_export(const RefConst & rc, const u32 * norm, u32 * words, u32 n, cudaStream_t s);
+cudaError_t launch_import(const RefConst & rc, const u32 * words, u32 * norm, u32 n, u32 * bad, cudaStream_t s);
 
 } // namespace ab

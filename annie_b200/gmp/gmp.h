@@ -109,6 +109,10 @@ void mpz_fdiv_r_2exp(mpz_ptr, mpz_srcptr, mp_bitcnt_t);
 void mpz_tdiv_q_2exp(mpz_ptr, mpz_srcptr, mp_bitcnt_t);
 #define mpz_mod __gmpz_mod
 void mpz_mod(mpz_ptr, mpz_srcptr, mpz_srcptr);
+#define mpz_fdiv_ui __gmpz_fdiv_ui
+unsigned long int mpz_fdiv_ui(mpz_srcptr, unsigned long int);
+#define mpz_divexact_ui __gmpz_divexact_ui
+void mpz_divexact_ui(mpz_ptr, mpz_srcptr, unsigned long int);
 /* Obsolete names kept by the manual: division rounding toward -infinity. */
 #define mpz_div_2exp mpz_fdiv_q_2exp
 #define mpz_mod_2exp mpz_fdiv_r_2exp

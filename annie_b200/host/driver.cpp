@@ -235,13 +235,8 @@ int run(const mpz_t n, const ab_prp_options & o, ab_prp_result & r)
 
 		if (!injected && (int64_t)i == o.inject_iteration)
 		{
-			// host-side fault: one residue of Reg0 moves by one, between two launches
-			const size_t words = (size_t)p.K << p.ln;
-			std::vector<uint32_t> reg(words);
-			if (ab_read_register(t.handle(), 0, reg.data(), words) != AB_OK) throw std::runtime_error(ab_last_error());
-			const size_t w = o.inject_word % words;
-			reg[w] = (reg[w] == 0) ? 1u : reg[w] - 1u;
-			if (ab_write_register(t.handle(), 0, reg.data(), words) != AB_OK) throw std::runtime_error(ab_last_error());
+			// host-side fault: one 32-bit word of Reg0 moves by one, between two launches
+			if (ab_inject_word(t.handle(), 0, o.inject_word, -1) != AB_OK) throw std::runtime_error(ab_last_error());
 			injected = true;
 		}
 

@@ -128,7 +128,9 @@ public:
 
 	std::string get_data_size() const override
 	{
-		const size_t bytes = (size_t)16 * _p.K * ((size_t)1 << _p.ln) * 4;
+		// 7 normal-form buffers (3 words per coefficient), 8 NTT-form buffers and
+		// 3 twiddle tables (K + 1 words), the reference-word staging (K words)
+		const size_t bytes = (size_t)(21 + 11 * (_p.K + 1) + _p.K) * ((size_t)1 << _p.ln) * 4;
 		std::ostringstream ss; ss << "data size: ";
 		if (bytes < (10u << 20)) ss << bytes / 1024 << " KB"; else ss << (bytes >> 20) << " MB";
 		return ss.str();
@@ -139,7 +141,7 @@ public:
 	std::string get_info_short() const override
 	{
 		std::ostringstream ss;
-		ss << _p.K << "-prime NTT of length " << (1u << _p.ln) << ", packed-base = 2^{" << _p.pck << "x" << _p.lbase << "}";
+		ss << _p.K + 1 << "-prime NTT of length " << (1u << _p.ln) << ", packed-base = 2^{" << _p.pck << "x" << _p.lbase << "}";
 		return ss.str();
 	}
 

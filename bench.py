@@ -651,13 +651,11 @@ def run_proth2m_workload(args):
     c0 = time.perf_counter()
     ok, stash = block_with_check()
     gl_ms = (time.perf_counter() - c0) * 1e3
-    # injected error: one residue word of Reg0 moves by one, mid-block
+    # injected error: one 32-bit word of Reg0 moves by one, mid-block
     verified_i = state["i"]
     c0 = time.perf_counter()
     run(B // 2)
-    reg = t.read_register(0)
-    reg[12345 % len(reg)] = (int(reg[12345 % len(reg)]) - 1) % (1 << 32)
-    t.write_register(0, reg)
+    t.inject_word(0, 12345, -1)
     bad, _ = block_with_check()
     t.read_checkpoint(stash)                              # roll back to the verified state
     state["i"] = verified_i
@@ -675,7 +673,7 @@ def run_proth2m_workload(args):
                        "l2": "256 MiB write before the timed region; the working set (about 10 MB) stays in L2"},
             "gl_check": {"ms": round(gl_ms, 2), "passed": bool(ok)},
             "injected_error": {"detected": not bad, "rolled_back_and_verified": bool(redo), "ms": round(rb_ms, 2),
-                               "note": "one Reg0 word changed by one mid-block; time from the change through the failed "
+                               "note": "one 32-bit word of Reg0 changed by one mid-block; time from the change through the failed "
                                        "check, the reload of the verified state and the repeated, verified block"}}
 
 

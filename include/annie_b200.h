@@ -78,10 +78,19 @@ int ab_read_checkpoint(ab_transform * h, const void * buf, size_t size);
 void * ab_host_alloc(size_t bytes);
 void ab_host_free(void * p);
 
-/* Raw register words (K planes of n u32, normal form) -- the engine's
-   read_memory / write_memory (engine.h of the reference). */
+/* Raw register words of the reference's normal form: K planes of n u32, the
+   residues of each coefficient's value mod the reference's primes -- the
+   engine's read_memory / write_memory (engine.h of the reference).  The
+   engine itself keeps each coefficient's exact value (three 32-bit limbs) and
+   converts on the device; ab_write_register returns AB_E_ARG when the words
+   are not those of a normal-form register (a coefficient beyond 96 bits). */
 int ab_read_register(ab_transform * h, size_t reg, uint32_t * out, size_t cap_words);
 int ab_write_register(ab_transform * h, size_t reg, const uint32_t * in, size_t nwords);
+
+/* Fault injection for the Gerbicz-Li tests (no counterpart in the reference):
+   adds delta to one 32-bit word (index mod 3 n) of the engine's own copy of
+   register reg, between two launches. */
+int ab_inject_word(ab_transform * h, size_t reg, size_t index, int32_t delta);
 
 /* Waits for all work queued on the handle's stream. */
 int ab_synchronize(ab_transform * h);
@@ -135,11 +144,12 @@ int ab_flush_l2(ab_transform * h, size_t bytes);
  * all device memory to its own allocator or pool at start-up, or a service
  * with a fixed memory budget.  Such a caller creates the handle (which
  * allocates) during start-up, and afterwards squares registers it owns:
- * reg_device = a caller-owned device array of K*n words in the normal
- * register layout; it is replaced by a * reg^2 in MMGW form, exactly as
- * ab_square_mul does for Reg0.  The work buffers come from a static device
- * array of 5 x 2^19 words (10 MiB) that every GPU loading this library holds
- * until exit, so K*n must not exceed 2^19 words (else AB_E_CAPACITY).  No
+ * reg_device = a caller-owned device array of K*n words, a normal-form
+ * register in the reference's layout (as ab_read_register gives it); it is
+ * replaced by a * reg^2 in MMGW form, exactly as ab_square_mul does for Reg0.
+ * The work buffers come from a static device array of 5 x 2^19 words
+ * (10 MiB) that every GPU loading this library holds until exit, so the NTT
+ * length must not exceed 2^16 (else AB_E_CAPACITY).  No
  * cudaMalloc, cudaFree or allocating library call is made: the array's device
  * address is looked up (cudaGetSymbolAddress, with the device current) when
  * the handle is created, so a call only queues kernels.  a must be >= 1
@@ -149,13 +159,17 @@ int ab_flush_l2(ab_transform * h, size_t bytes);
  * handles' streams, other host threads) race and give wrong results. */
 int ab_square_mul_noalloc(ab_transform * h, uint32_t * reg_device, int32_t a);
 
-/* Diagnostics (kernel-level parity tests): run one stage on host data.
-   ab_diag_forward:  full forward NTT of a normal-form register (domain 0 = R, 1 = Q).
-   ab_diag_product:  forward NTT, pointwise square (xp == NULL) or product with the
-                     forward image xp, inverse NTT, carry (a, nega for domain Q,
+/* Diagnostics (kernel-level parity tests): run one stage on host data; inputs
+   and the product's output are normal-form registers in the reference's
+   layout (K planes).  They use the handle's work buffers (registers kept).
+   ab_diag_forward:  full forward NTT of a register (domain 0 = R, 1 = Q) over
+                     the engine's own transform primes: (K+1) planes of n
+                     lazily reduced residues.
+   ab_diag_product:  forward NTT, pointwise square (y == NULL) or product with
+                     register y, inverse NTT, carry (a, nega for domain Q,
                      optional subtraction, lower_mode 0 none / 1 mod R + 2 / 2 mod Q). */
 int ab_diag_forward(ab_transform * h, int domain, const uint32_t * in, uint32_t * out);
-int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * xp,
+int ab_diag_product(ab_transform * h, int domain, const uint32_t * in, const uint32_t * y,
 	uint32_t a, const uint32_t * sub, int lower_mode, uint32_t * out);
 
 #ifdef __cplusplus

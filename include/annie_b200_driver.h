@@ -21,7 +21,7 @@ typedef struct
 	int device;
 	int gl_check_blocks;       /* verify the Gerbicz-Li product every this many blocks of B squarings; 0 = final check only */
 	int64_t inject_iteration;  /* flip one word of Reg0 right after this loop index (bit of the exponent); -1 = none */
-	uint32_t inject_word;      /* index (mod K n) of the word to flip */
+	uint32_t inject_word;      /* index (mod 3 n) of the word of Reg0 to change (ab_inject_word) */
 	const char * checkpoint_path;  /* NULL: no checkpoint files; else saved every checkpoint_seconds and on abort (annie.h:162-190) */
 	double checkpoint_seconds;
 	int verbose;

@@ -25,20 +25,20 @@ def pick_N(bits, seed, a=3, rule_cpu_too=False, oracle=None):
     raise RuntimeError("no N found")
 
 
-def random_digits_register(K, pck, ln, lbase, seed):
+def random_digits_register(K, pck, ln, lbase, seed, with_exact=False):
     """Normal-form register of random digits: coefficient i holds the residues
-    of D_i = sum_l d_l 2^(l lbase), d_l uniform in [0, 2^lbase)."""
+    of D_i = sum_l d_l 2^(l lbase), d_l uniform in [0, 2^lbase) (and, with
+    with_exact, the D_i)."""
     rng = np.random.default_rng(seed)
     n = 1 << ln
     d = [rng.integers(0, 1 << lbase, size=n, dtype=np.uint64) for _ in range(pck)]
+    v = np.zeros(n, dtype=object)
+    for l in reversed(range(pck)):
+        v = v * (1 << lbase) + d[l].astype(object)
     out = np.zeros(K * n, dtype=np.uint32)
     for k in range(K):
-        p = PRIMES[k]
-        v = np.zeros(n, dtype=object)
-        for l in reversed(range(pck)):
-            v = v * (1 << lbase) + d[l].astype(object)
-        out[k * n:(k + 1) * n] = np.array([int(x) % p for x in v], dtype=np.uint32)
-    return out
+        out[k * n:(k + 1) * n] = np.array([int(x) % PRIMES[k] for x in v], dtype=np.uint32)
+    return (out, list(v)) if with_exact else out
 
 
 def random_residues(K, ln, seed):

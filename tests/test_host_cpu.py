@@ -8,7 +8,6 @@ import os
 import sys
 import types
 
-import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
@@ -69,8 +68,7 @@ class _ExactTransform:
     def get(self, i): return self.r[i]
     def save_checkpoint(self): return (self.r[0], self.r[1])
     def read_checkpoint(self, p): self.r[0], self.r[1] = p; return True
-    def read_register(self, i): return np.zeros(16, dtype=np.uint32)
-    def write_register(self, i, words): self.r[i] = (self.r[i] + 1) % self.N    # one word moved
+    def inject_word(self, i, index, delta=-1): self.r[i] = (self.r[i] + 1) % self.N    # one word moved
     def synchronize(self): pass
     def flush_l2(self, n): pass
     def timer_start(self): pass
