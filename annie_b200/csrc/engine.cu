@@ -98,22 +98,22 @@ size_t bitrev(size_t i, size_t n)
 	return r;
 }
 
-// Twiddle tables of transform prime k for length 2^ln, as Shoup pairs
-// (w, floor(w 2^32 / p)) at the reference's positions s + bitrev(j, s),
-// s = n/4 .. 1 (transformGPU.h:117-160; position 0 unused).  Domain R
-// (x^n - 1): w = rho_s^j with rho_s a primitive 2s-th root of unity, and
-// wi = -rho_s^-j.  Domain Q (x^n + 1), twisted: w = psi_s rho_s^j with psi_s a
-// primitive 4s-th root (psi_s^2 = rho_s); it needs no inverse table, since
-// -w_j^-1 = w_{s-1-j}, which sits at the mirrored position.
-void make_twiddles(uint2 * w, uint2 * wi, int ln, int k, bool domain_q)
+// Twiddles of transform prime k for length 2^ln at the reference's positions
+// s + bitrev(j, s), s = n/4 .. 1 (transformGPU.h:117-160; position 0 unused).
+// Domain R (x^n - 1): w = rho_s^j with rho_s a primitive 2s-th root of unity;
+// the inverse levels use -rho_s^-j.  Domain Q (x^n + 1), twisted:
+// w = psi_s rho_s^j with psi_s a primitive 4s-th root (psi_s^2 = rho_s), and
+// -w_j^-1 = w_{s-1-j}, the forward twiddle at the mirrored position.
+// Outputs, as Shoup pairs (w, floor(w 2^32 / p)): the row tables (w, and wi
+// for domain R only), and the column tables (the first COLTW positions),
+// forward cf and inverse ci (both domains).
+void make_twiddles(uint2 * w, uint2 * wi, uint2 * cf, uint2 * ci, int ln, int k, bool domain_q)
 {
 	const TZp z(TPRIMES[k]);
-	const size_t n = (size_t)1 << ln;
+	const size_t n = (size_t)1 << ln, h = n / 2, nc = std::min<size_t>(h, COLTW);
 	auto root = [&](int l) { return z.pow(TGEN[k], (z.p - 1) >> l); };     // primitive 2^l-th root
-	auto pair = [&](u32 v) { return make_uint2(v, z.shoup(v)); };
-	w[0] = make_uint2(0, 0);
-	if (wi) wi[0] = make_uint2(0, 0);
-	int l = ln - 1;                                  // rho of the level s = n/4 has order 2^(ln-1)
+	std::vector<u32> fw(h, 0), iw(h, 0);                  // plain values
+	int l = ln - 1;                                       // rho of the level s = n/4 has order 2^(ln-1)
 	for (size_t s = n / 4; s >= 1; s /= 2, --l)
 	{
 		const u32 rho = root(l), rhoi = z.inv(rho);
@@ -121,10 +121,24 @@ void make_twiddles(uint2 * w, uint2 * wi, int ln, int k, bool domain_q)
 		for (size_t j = 0; j < s; ++j)
 		{
 			const size_t jr = bitrev(j, s);
-			w[s + jr] = pair(t);
-			if (wi) wi[s + jr] = pair((z.p - ti) % z.p);
+			fw[s + jr] = t;
+			iw[s + jr] = (z.p - ti) % z.p;
 			t = z.mul(t, rho); ti = z.mul(ti, rhoi);
 		}
+	}
+	if (domain_q)
+		for (size_t s = n / 4; s >= 1; s /= 2)
+			for (size_t i = s; i < 2 * s; ++i) iw[i] = fw[3 * s - 1 - i];     // -w^-1 (same values as above)
+	for (size_t i = 0; i < h; ++i)
+	{
+		w[i] = make_uint2(fw[i], z.shoup(fw[i]));
+		if (wi) wi[i] = make_uint2(iw[i], z.shoup(iw[i]));
+	}
+	for (size_t i = 0; i < COLTW; ++i)
+	{
+		const u32 a = (i < nc) ? fw[i] : 0u, bb = (i < nc) ? iw[i] : 0u;
+		cf[i] = make_uint2(a, z.shoup(a));
+		ci[i] = make_uint2(bb, z.shoup(bb));
 	}
 }
 
@@ -221,10 +235,11 @@ struct ab_transform
 	// Gerbicz-Li snapshot.  NTT form (KP planes): the four partly transformed
 	// work buffers, the transforms of N (domain Q) and N^-1 (domain R), two
 	// transformed multiplicands.  Shared by the slots of a batch: XW (the
-	// reference's register words, K planes, for conversions) and the twiddle
-	// tables (KP n words each: n/2 Shoup pairs per prime).
+	// reference's register words, K planes, for conversions), the row twiddle
+	// tables (KP n/2 words each) and the column twiddle tables (WC: domains R,
+	// Q x forward, inverse x KP primes x COLTW Shoup pairs).
 	enum Buf { REG0 = 0, REG1, REG2, ONE, TQ, TMP, SNAP, AQ0, AQ1, AR0, AR1, NQ, NIR, OPQ, OPR, NSLOT = OPR + 1,
-	           XW = NSLOT, WR, WRI, WQ, NBUF };
+	           XW = NSLOT, WR, WRI, WQ, WC, NBUF };
 	static bool normal_buf(int i) { return i <= SNAP; }
 
 	int device = 0;
@@ -266,12 +281,14 @@ struct ab_transform
 	int mult_i = 0;
 
 	u32 * b(int i) const { return bufp[i]; }
-	const uint2 * tw(int i) const { return reinterpret_cast<const uint2 *>(bufp[i]); }
-	size_t words_of(int i) const
+	static size_t words_of(int i, int K, size_t n)
 	{
-		if (i == XW) return (size_t)prm.K * n;
-		return (i < NSLOT && normal_buf(i)) ? (size_t)AB_NW * n : (size_t)KP * n;
+		if (i == XW) return (size_t)K * n;
+		if (i == WR || i == WRI || i == WQ) return (size_t)(K + 1) * n;        // n/2 pairs per prime
+		if (i == WC) return (size_t)4 * (K + 1) * COLTW * 2;
+		return (i < NSLOT && normal_buf(i)) ? (size_t)AB_NW * n : (size_t)(K + 1) * n;
 	}
+	size_t words_of(int i) const { return words_of(i, prm.K, n); }
 
 	ab_transform() { mpz_inits(N, factor, nullptr); }
 	ab_transform(const ab_transform &) = delete;
@@ -432,9 +449,11 @@ struct ab_transform
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, s));
 		++launches;
 	}
-	// twiddles of a domain (q: Q, else R)
-	const uint2 * wf(bool q) const { return tw(q ? WQ : WR); }
-	const uint2 * wv(bool q) const { return q ? nullptr : tw(WRI); }
+	// twiddles of a domain (q: Q, else R): row tables, and the column tables
+	// (forward, inverse) of WC
+	const uint2 * wf(bool q) const { return reinterpret_cast<const uint2 *>(b(q ? WQ : WR)); }
+	const uint2 * wv(bool q) const { return q ? nullptr : reinterpret_cast<const uint2 *>(b(WRI)); }
+	const uint2 * wc(bool q, bool inverse) const { return reinterpret_cast<const uint2 *>(b(WC)) + ((q ? 2 : 0) + (inverse ? 1 : 0)) * KP * COLTW; }
 	RowJob rj(u32 * x, int mode, bool q, const u32 * xp = nullptr) const
 	{
 		RowJob j; std::memset(&j, 0, sizeof(j)); j.x = x; j.xp = xp; j.w = wf(q); j.wi = wv(q); j.mode = mode; return j;
@@ -446,13 +465,13 @@ struct ab_transform
 	ColJob cj_tr(const u32 * in, bool q, u32 a, const u32 * sub, int lower) const
 	{
 		ColJob j; std::memset(&j, 0, sizeof(j));
-		j.in = in; j.transformed = 1; j.w_in = wf(q); j.wi_in = wv(q); j.a = a; j.nega = q ? 1 : 0; j.sub = sub; j.lower = lower;
+		j.in = in; j.transformed = 1; j.wi_in = wc(q, true); j.a = a; j.nega = q ? 1 : 0; j.sub = sub; j.lower = lower;
 		return j;
 	}
 	void set_fwd(ColJob & j, u32 * q_out, u32 * r_out) const
 	{
-		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wf(true) : nullptr;
-		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wf(false) : nullptr;
+		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wc(true, false) : nullptr;
+		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wc(false, false) : nullptr;
 	}
 
 	// full forward transform of a normal-form register in one or two domains
@@ -700,17 +719,32 @@ struct ab_transform
 		CK(cudaStreamSynchronize(st));
 	}
 
-	// twiddle tables of the class (host), KP n words per table
-	static void twiddle_tables(const ab_params & prm, std::vector<uint2> & wr, std::vector<uint2> & wri, std::vector<uint2> & wq)
+	// twiddle tables of the class (host): row tables WR, WRI, WQ (KP n/2 pairs
+	// each) and the column tables WC
+	static void twiddle_tables(const ab_params & prm, std::vector<uint2> & wr, std::vector<uint2> & wri, std::vector<uint2> & wq,
+	                           std::vector<uint2> & wc)
 	{
 		const size_t h = (size_t)1 << (prm.ln - 1);
 		const int KP = prm.K + 1;
 		wr.assign(KP * h, make_uint2(0, 0)); wri.assign(KP * h, make_uint2(0, 0)); wq.assign(KP * h, make_uint2(0, 0));
+		wc.assign((size_t)4 * KP * COLTW, make_uint2(0, 0));
 		for (int k = 0; k < KP; ++k)
 		{
-			make_twiddles(&wr[k * h], &wri[k * h], prm.ln, k, false);
-			make_twiddles(&wq[k * h], nullptr, prm.ln, k, true);
+			uint2 * const c = wc.data();
+			make_twiddles(&wr[k * h], &wri[k * h], c + (0 * KP + k) * COLTW, c + (1 * KP + k) * COLTW, prm.ln, k, false);
+			make_twiddles(&wq[k * h], nullptr, c + (2 * KP + k) * COLTW, c + (3 * KP + k) * COLTW, prm.ln, k, true);
 		}
+	}
+
+	void upload_twiddles()
+	{
+		std::vector<uint2> wr, wri, wq, wcv;
+		twiddle_tables(prm, wr, wri, wq, wcv);
+		CK(cudaMemcpyAsync(b(WR), wr.data(), wr.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(WRI), wri.data(), wri.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(WQ), wq.data(), wq.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(b(WC), wcv.data(), wcv.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+		CK(cudaStreamSynchronize(st));
 	}
 
 	void init(const mpz_t Nin, int32_t a, int dev, const ab_params * forced)
@@ -736,12 +770,7 @@ struct ab_transform
 		for (int i = 0; i < NBUF; ++i) bufp[i] = dmem + offs[i];
 
 		host.assign((size_t)AB_NW * n, 0);
-		std::vector<uint2> wr, wri, wq;
-		twiddle_tables(prm, wr, wri, wq);
-		CK(cudaMemcpyAsync(b(WR), wr.data(), wr.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
-		CK(cudaMemcpyAsync(b(WRI), wri.data(), wri.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
-		CK(cudaMemcpyAsync(b(WQ), wq.data(), wq.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
-		CK(cudaStreamSynchronize(st));
+		upload_twiddles();
 		setup_device(pp);
 	}
 };
@@ -793,6 +822,10 @@ struct ab_batch
 	u32 * ctrl(int step, int part) const { return d_ctrl + ((size_t)step * 3 + part) * cap; }
 	const uint2 * wf(bool q) const { return reinterpret_cast<const uint2 *>(base[q ? ab_transform::WQ : ab_transform::WR]); }
 	const uint2 * wv(bool q) const { return q ? nullptr : reinterpret_cast<const uint2 *>(base[ab_transform::WRI]); }
+	const uint2 * wc(bool q, bool inverse) const
+	{
+		return reinterpret_cast<const uint2 *>(base[ab_transform::WC]) + ((q ? 2 : 0) + (inverse ? 1 : 0)) * (cls.K + 1) * COLTW;
+	}
 
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
@@ -814,15 +847,15 @@ struct ab_batch
 	{
 		ColJob j; std::memset(&j, 0, sizeof(j));
 		j.in = in; j.transformed = tr ? 1 : 0;
-		if (tr) { j.w_in = wf(q); j.wi_in = wv(q); j.nega = q ? 1 : 0; }
+		if (tr) { j.wi_in = wc(q, true); j.nega = q ? 1 : 0; }
 		j.a = 1; j.mult = mult; j.sub = sub;
 		j.lower = lower; j.stride_ntt = w_ntt; j.stride_norm = w_norm; j.cand = d_cand;
 		return j;
 	}
 	void set_fwd(ColJob & j, u32 * q_out, u32 * r_out) const
 	{
-		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wf(true) : nullptr;
-		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wf(false) : nullptr;
+		j.out_fwd[0] = q_out; j.w_out[0] = q_out ? wc(true, false) : nullptr;
+		j.out_fwd[1] = r_out; j.w_out[1] = r_out ? wc(false, false) : nullptr;
 	}
 
 	// squareMMGW (transformGPU.h:556-568) for every slot, `steps` times
@@ -1103,7 +1136,10 @@ int ab_write_register(ab_transform * h, size_t reg, const uint32_t * in, size_t 
 
 int ab_synchronize(ab_transform * h)
 {
-	return guarded([&] { if (h == nullptr) throw ab_error(AB_E_ARG, "null handle"); if (h->st) CK(cudaStreamSynchronize(h->st)); });
+	return guarded([&] {
+		if (h == nullptr) throw ab_error(AB_E_ARG, "null handle");
+		if (h->st) CK(cudaStreamSynchronize(h->st));
+	});
 }
 
 int ab_timer_start(ab_transform * h)
@@ -1292,19 +1328,19 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 		for (int i = 0; i < ab_transform::NBUF; ++i)
 		{
 			offs[i] = total;
-			const size_t w = (i < ab_transform::NSLOT) ? b->slot_words(i) * capacity
-			               : (i == ab_transform::XW) ? (size_t)cls->K * b->n : b->w_ntt;
+			const size_t w = (i < ab_transform::NSLOT) ? b->slot_words(i) * capacity : ab_transform::words_of(i, cls->K, b->n);
 			total += (w + 63) / 64 * 64;
 		}
 		CK(cudaMalloc(&b->mem, total * 4));
 		CK(cudaMemsetAsync(b->mem, 0, total * 4, b->st));
 		b->d_flag = b->mem;
 		for (int i = 0; i < ab_transform::NBUF; ++i) b->base[i] = b->mem + offs[i];
-		std::vector<uint2> wr, wri, wq;
-		ab_transform::twiddle_tables(*cls, wr, wri, wq);
+		std::vector<uint2> wr, wri, wq, wcv;
+		ab_transform::twiddle_tables(*cls, wr, wri, wq, wcv);
 		CK(cudaMemcpyAsync(b->base[ab_transform::WR], wr.data(), wr.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
 		CK(cudaMemcpyAsync(b->base[ab_transform::WRI], wri.data(), wri.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
 		CK(cudaMemcpyAsync(b->base[ab_transform::WQ], wq.data(), wq.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
+		CK(cudaMemcpyAsync(b->base[ab_transform::WC], wcv.data(), wcv.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->st));
 		CK(cudaMalloc(&b->d_cand, sizeof(CandConst) * capacity));
 		b->h_cand.assign(capacity, CandConst{});
 		for (auto & c : b->h_cand) c.lbase = 2;

@@ -200,16 +200,24 @@ __device__ __forceinline__ void reduce_all(u32 (&v)[N], u32 p2)
 // is compiled for 4 CTAs per SM (at most 64 registers), so that the Q- and
 // R-domain row passes, which run side by side on two streams, are resident
 // together.
+#ifndef AB_ROW_THREADS
+#define AB_ROW_THREADS 256
+#endif
+#ifndef AB_ROW_MINB
+#define AB_ROW_MINB 4
+#endif
 template <int LOG_R>
 struct RowCfg
 {
 	static constexpr u32 T = (1u << LOG_R) / RP_EPT;             // virtual threads
-	static constexpr u32 NT = (T < 256u) ? T : 256u;             // physical threads
+	static constexpr u32 NT = (T < AB_ROW_THREADS) ? T : AB_ROW_THREADS;   // physical threads
 	static constexpr u32 RND = T / NT;
+	static constexpr int MINB = (AB_ROW_MINB * AB_ROW_THREADS > 2048) ? 2048 / AB_ROW_THREADS : AB_ROW_MINB;
+	static constexpr size_t SMEM = sizeof(u32) * ((1u << LOG_R) + (1u << LOG_R) / 16);   // padded row
 };
 
 template <int LOG_R>
-__global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs jobs, const TConst c)
+__global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowpass(const RowJobs jobs, const TConst c)
 {
 	constexpr int LB = LOG_R - 1;
 	constexpr u32 T = RowCfg<LOG_R>::T, NT = RowCfg<LOG_R>::NT, RND = RowCfg<LOG_R>::RND;
@@ -332,7 +340,10 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, 4) k_rowpass(const RowJobs 
 
 // ================================================================ column pass
 constexpr int CC = 32;  // own columns per CTA
-constexpr int COL_THREADS = 384;
+#ifndef AB_COL_THREADS
+#define AB_COL_THREADS 384
+#endif
+constexpr int COL_THREADS = AB_COL_THREADS;
 constexpr int TW = 40;  // tile row stride: own columns + up to 8 predecessor columns
 
 // One radix-2^S step of the column transform (levels on row bits b..b+S-1)
@@ -373,15 +384,30 @@ __device__ __forceinline__ void col_step(u32 * __restrict__ colp, int LOG_H, int
 	for (int g = 0; g < (1 << S); ++g) base[g * D] = v[g];
 }
 
-// All LOG_H levels of the columns u in [u0, u0 + nu) of every prime, in place
-// in the tile; stages of 3 levels (the remainder first in the forward order).
-template <int LOG_H, int KP, bool INV>
-__device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const uint2 * twk, const TConst & c)
+// One task of a column stage: column u of prime k, row group o.
+template <int LOG_H, bool INV>
+__device__ __forceinline__ void col_task(u32 * tile, int u, int o, int k, int S, int b, const uint2 * twk, const TConst & c)
 {
-	constexpr int H = 1 << LOG_H;
+	u32 * colp = tile + (k << LOG_H) * TW + u;
+	const uint2 * tw = twk + (k << LOG_H);
+	const u32 p = c.p[k];
+	if (S == 3) col_step<3, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
+	else if (S == 2) col_step<2, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
+	else col_step<1, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
+}
+
+// All LOG_H levels of the CC own columns [E, E + CC) and, with pred, the E
+// predecessor columns [0, E) of every prime, in place in the tile; stages of
+// 3 levels (the remainder first in the forward order).  Task indices split
+// by shifts only (E is 0, 4 or 8).
+template <int LOG_H, int KP, bool INV>
+__device__ __forceinline__ void col_transform(u32 * tile, int E, bool pred, const uint2 * twk, const TConst & c)
+{
 	constexpr int SR = (LOG_H % 3 == 0) ? 3 : LOG_H % 3;       // top stage (row bits LOG_H-SR..LOG_H-1)
 	constexpr int NST = 1 + (LOG_H - SR) / 3;
+	static_assert(CC == 32, "32 own columns per CTA");
 	const int tid = (int)threadIdx.x, NT = (int)blockDim.x;
+	const int le = (E == 8) ? 3 : 2;                           // log2 E when E > 0
 #pragma unroll 1
 	for (int st = 0; st < NST; ++st)
 	{
@@ -390,19 +416,12 @@ __device__ __forceinline__ void col_transform(u32 * tile, int u0, int nu, const 
 		const bool top = (idx == 0);
 		const int b = top ? (LOG_H - SR) : (LOG_H - SR - 3 * idx);
 		const int S = top ? SR : 3;
-		const int ntask = KP * nu * (H >> S);
-		for (int task = tid; task < ntask; task += NT)
-		{
-			const int u = u0 + task % nu;
-			const int rest = task / nu;
-			const int o = rest % (H >> S), k = rest / (H >> S);
-			u32 * colp = tile + (k * H) * TW + u;
-			const uint2 * tw = twk + k * H;
-			const u32 p = c.p[k];
-			if (S == 3) col_step<3, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
-			else if (S == 2) col_step<2, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
-			else col_step<1, INV>(colp, LOG_H, b, (u32)o, tw, p, 2 * p);
-		}
+		const int lo = LOG_H - S;                                // log2 of the row groups
+		for (int task = tid; task < (KP << (lo + 5)); task += NT)
+			col_task<LOG_H, INV>(tile, E + (task & 31), (task >> 5) & ((1 << lo) - 1), task >> (lo + 5), S, b, twk, c);
+		if (pred && E > 0)
+			for (int task = tid; task < (KP << (lo + le)); task += NT)
+				col_task<LOG_H, INV>(tile, task & (E - 1), (task >> le) & ((1 << lo) - 1), task >> (lo + le), S, b, twk, c);
 		__syncthreads();
 	}
 }
@@ -526,25 +545,29 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	// ---- load the tile (NTT form: KP planes; normal form: the three limb
 	// planes) and the column twiddles
 	const int np_in = J.transformed ? KP : AB_NW;
-	for (int idx = tid; idx < np_in * H * ng; idx += NT)
+	for (int idx = tid; idx < (np_in << (LOG_H + 3)); idx += NT)
 	{
-		const int u4 = idx % ng, row = (idx / ng) % H, k = idx / (ng * H);
-		const uint4 val = __ldg(reinterpret_cast<const uint4 *>(J.in + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
-		*reinterpret_cast<uint4 *>(tile + k * PS + row * TW + 4 * u4) = val;
+		const int u4 = idx & 7, row = (idx >> 3) & (H - 1), k = idx >> (LOG_H + 3);
+		const uint4 val = __ldg(reinterpret_cast<const uint4 *>(J.in + (size_t)k * n + (size_t)row * R + c0 + 4 * u4));
+		*reinterpret_cast<uint4 *>(tile + k * PS + row * TW + E + 4 * u4) = val;
 	}
-	const size_t hn = n >> 1;                    // twiddle pairs per prime
+	if (E > 0)
+	{
+		const int le4 = (E == 8) ? 1 : 0;                          // log2 of the predecessor groups
+		for (int idx = tid; idx < (np_in << (LOG_H + le4)); idx += NT)
+		{
+			const int u4 = idx & (E / 4 - 1), row = (idx >> le4) & (H - 1), k = idx >> (LOG_H + le4);
+			const uint4 val = __ldg(reinterpret_cast<const uint4 *>(J.in + (size_t)k * n + (size_t)row * R + gcol(4 * u4)));
+			*reinterpret_cast<uint4 *>(tile + k * PS + row * TW + 4 * u4) = val;
+		}
+	}
 	for (int idx = tid; idx < KP * H; idx += NT)
 	{
 		const int k = idx / H, i = idx % H;
 		if (i == 0) continue;
-		if (J.transformed)
-		{
-			// -w^-1 of the source domain: its own table (R) or the mirror of w (Q)
-			const int s = 1 << (31 - __clz(i));
-			twc[idx] = (J.wi_in != nullptr) ? J.wi_in[(size_t)k * hn + i] : J.w_in[(size_t)k * hn + (3 * s - 1 - i)];
-		}
-		if (J.out_fwd[0] != nullptr) twc[KP * H + idx] = J.w_out[0][(size_t)k * hn + i];
-		if (J.out_fwd[1] != nullptr) twc[2 * KP * H + idx] = J.w_out[1][(size_t)k * hn + i];
+		if (J.transformed) twc[idx] = J.wi_in[k * COLTW + i];
+		if (J.out_fwd[0] != nullptr) twc[KP * H + idx] = J.w_out[0][k * COLTW + i];
+		if (J.out_fwd[1] != nullptr) twc[2 * KP * H + idx] = J.w_out[1][k * COLTW + i];
 	}
 	if (tid == 0) decision = 0;
 	__syncthreads();
@@ -552,14 +575,21 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	if (J.transformed)
 	{
 		// ---- inverse column levels (all WU columns, KP primes)
-		col_transform<LOG_H, KP, true>(tile, 0, WU, twc, c);
+		col_transform<LOG_H, KP, true>(tile, E, true, twc, c);
 
 		// ---- carry phase 1: per group, exact values (CRT), x a, - sub,
 		// unsigned digits + carry-out
-		for (int idx = tid; idx < H * ng; idx += NT)
+		const int npg = (E == 8) ? H + 1 : (E == 4) ? H : 0;    // predecessor groups carried (for E = 8 only row H-1's first)
+		for (int idx = tid; idx < H * (CC / 4) + npg; idx += NT)
 		{
-			const int row = idx / ng, u4 = idx % ng;
-			if (E == 8 && u4 == 0 && row != H - 1) continue;
+			int row, u4;
+			if (idx < H * (CC / 4)) { row = idx >> 3; u4 = E / 4 + (idx & 7); }
+			else
+			{
+				const int q = idx - H * (CC / 4);
+				if (E == 4) { row = q; u4 = 0; }
+				else { row = (q < H) ? q : H - 1; u4 = (q < H) ? 1 : 0; }
+			}
 			u32 xv[KP][4];
 #pragma unroll
 			for (int k = 0; k < KP; ++k)
@@ -700,7 +730,7 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 			encode4<KP>(c, l, tp, PS);
 		}
 		__syncthreads();
-		col_transform<LOG_H, KP, false>(tile, E, CC, twc + (1 + dom) * KP * H, c);
+		col_transform<LOG_H, KP, false>(tile, E, false, twc + (1 + dom) * KP * H, c);
 		for (int idx = tid; idx < KP * H * (CC / 4); idx += NT)
 		{
 			const int u4 = idx % (CC / 4), row = (idx / (CC / 4)) % H, k = idx / ((CC / 4) * H);
@@ -828,8 +858,7 @@ static cudaError_t allow_dynamic_smem(Kernel kernel, size_t smem, std::atomic<un
 template <int LOG_R>
 static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
-	const u32 R = 1u << LOG_R;
-	const size_t smem = sizeof(u32) * (R + R / 16);
+	const size_t smem = RowCfg<LOG_R>::SMEM;
 	static std::atomic<unsigned long long> attr_done{0};
 	const cudaError_t e = allow_dynamic_smem(k_rowpass<LOG_R>, smem, attr_done);
 	if (e != cudaSuccess) return e;

@@ -13,11 +13,13 @@
 //       square / multiply, and the inverse of those LB levels, one CTA per row.
 // * Normal form: AB_NW = 3 planes of n words, the limbs (low first) of each
 //   coefficient's exact value in two's complement.
-// * Twiddles of one domain and prime: forward table w of n/2 Shoup pairs
-//   (w, floor(w 2^32/p)) at the reference's bit-reversed positions (level
-//   with s polynomials: index s + bitrev(j, s), s = n/4 .. 1); domain R also
-//   has a table of -w^-1 at the same positions.  Domain Q needs none: there
-//   -w_j^-1 = w_{s-1-j}, the forward twiddle at the mirrored position.
+// * Twiddles of one domain and prime, at the reference's bit-reversed
+//   positions (level with s polynomials: index s + bitrev(j, s), s = n/4 .. 1):
+//     - row tables: n/2 Shoup pairs (w, floor(w 2^32/p)), forward w; domain R
+//       also has -w^-1.  Domain Q needs no inverse table: there
+//       -w_j^-1 = w_{s-1-j}, the forward twiddle at the mirrored position.
+//     - column tables: the first COLTW positions (the column levels), forward
+//       and -w^-1, for both domains, as Shoup pairs.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -28,6 +30,8 @@ namespace ab
 
 enum RowMode { ROW_FWD_ONLY = 0, ROW_SQUARE = 1, ROW_MUL = 2 };
 
+constexpr int COLTW = 128;   // column-table positions per prime (covers H <= 64 and its mirror)
+
 // Batches: blockIdx.z selects a candidate; its buffers are at +z*stride
 // words (twiddles are shared).  `active` (nullable) holds one word per
 // candidate, 0 = skip it.
@@ -35,8 +39,8 @@ struct RowJob
 {
 	u32 * x;          // KP x n buffer, rows transformed in place
 	const u32 * xp;   // ROW_MUL: full forward image of the other operand (same layout)
-	const uint2 * w;  // forward twiddles of the domain: per prime n/2 pairs
-	const uint2 * wi; // domain R: -w^-1 table (n/2 pairs per prime); null = domain Q (mirrored w)
+	const uint2 * w;  // row table of the domain: per prime n/2 Shoup pairs
+	const uint2 * wi; // domain R: its -w^-1 row table; null = domain Q (mirrored w)
 	int mode;
 	size_t stride;    // words between candidates (x and xp)
 	const u32 * active;
@@ -49,15 +53,14 @@ struct ColJob
 {
 	const u32 * in;      // source buffer
 	int transformed;     // 1: NTT-form source awaiting the inverse column levels + carry; 0: normal form
-	const uint2 * w_in;  // forward twiddles of the source domain (transformed source)
-	const uint2 * wi_in; // its -w^-1 table (domain R) or null (domain Q)
+	const uint2 * wi_in; // column table -w^-1 of the source domain (transformed source), COLTW pairs per prime
 	u32 a;               // carry: multiply by a
 	int nega;            // carry: wrap-around negated (mod x^n + 1)
 	const u32 * sub;     // carry: subtract this normal-form register (nullable)
 	int lower;           // LowerMode applied after the carry
 	u32 * out_norm;      // normal-form result (nullable)
 	u32 * out_fwd[2];    // first LA forward levels of the result, per domain (nullable)
-	const uint2 * w_out[2];
+	const uint2 * w_out[2];  // forward column tables of the output domains
 	size_t stride_ntt;   // words between candidates of NTT-form buffers (in when transformed, out_fwd)
 	size_t stride_norm;  // words between candidates of normal-form buffers (in when not, sub, out_norm, out_snap)
 	const u32 * mult;    // per candidate: the carry multiplier a, 0 = inactive (nullable: use `a`)

@@ -4,8 +4,8 @@ reduced butterflies, the Montgomery pointwise product and the CRT with its
 fixed-point quotient estimate, level by level.  Every element goes through the
 same operations in the same order as in the CUDA passes (only the grouping of
 butterflies into passes differs), so the model reproduces the device's lazy
-words exactly; it is the reference for the forward-transform kernel test and,
-on the CPU, checks the design against exact big-integer convolutions.
+words; it is the reference for the forward-transform kernel test and, on the
+CPU, checks the design against exact big-integer convolutions.
 """
 import numpy as np
 
