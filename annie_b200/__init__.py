@@ -60,6 +60,20 @@ class PrpResult(C.Structure):
         return d
 
 
+class BenchRow(C.Structure):
+    _fields_ = [("e", C.c_uint64), ("digits", C.c_int64), ("K", C.c_int), ("pck", C.c_int), ("ln", C.c_int),
+                ("lbase", C.c_int), ("validated", C.c_int), ("squarings", C.c_int64), ("ms_per_bit", C.c_double),
+                ("estimated_seconds", C.c_double)]
+
+    def asdict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# the sizes of the reference's benchmark table (src/annie.h:448): N = 3 2^e + 1
+BENCH_TABLE_E = [33216, 83048, 166092, 332190, 664381, 1162672, 1660962, 3321924, 6643854, 16609638, 33219278,
+                 66438557, 159200000]
+
+
 class RunnerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots_per_class", C.c_int), ("chunk", C.c_int),
                 ("autotune", C.c_int)]
@@ -107,6 +121,7 @@ ABI = [
     ("ab_prp_check", [_u64p, C.c_size_t, C.POINTER(PrpOptions), C.POINTER(PrpResult)], C.c_int),
     ("ab_prp_quit", [], None),
     ("ab_prp_reset_quit", [], None),
+    ("ab_bench_table", [C.c_int, _u64p, C.c_int, C.c_double, C.POINTER(BenchRow)], C.c_int),
     ("ab_batch_slot_bytes", [C.POINTER(Params)], C.c_size_t),
     ("ab_batch_create", [C.c_int, C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     ("ab_batch_destroy", [C.c_void_p], None),
@@ -195,6 +210,18 @@ def prp_check(N, euler=False, base=0, device=0, gl_check_blocks=0, inject_iterat
     limbs = int_to_limbs(N)
     L.ab_prp_check(limbs.ctypes.data_as(_u64p), len(limbs), C.byref(o), C.byref(r))
     return r.asdict()
+
+
+def bench_table(e_list=None, seconds=10.0, device=0):
+    """The reference's benchmark mode (annie::bench, src/annie.h:432-556): one
+    row per N = 3 2^e + 1 (dicts), stopping after a row that does not validate."""
+    e_list = BENCH_TABLE_E if e_list is None else list(e_list)
+    es = np.array(e_list, dtype=np.uint64)
+    rows = (BenchRow * len(e_list))()
+    done = lib().ab_bench_table(device, es.ctypes.data_as(_u64p), len(e_list), seconds, rows)
+    if done < 0:
+        raise EngineError(AB_E_CUDA, "ab_bench_table failed")
+    return [rows[i].asdict() for i in range(done)]
 
 
 class Transform:

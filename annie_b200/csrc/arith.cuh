@@ -83,8 +83,9 @@ struct TConst
 	u32 negm[AB_MAXK];                   // -M mod 2^(32 L)
 	int K, KP, pck, lbase, ln;           // reference primes K, transform primes KP = K + 1
 	u32 n;                               // 2^ln
-	u32 R, H;                            // row length and row count of the 2-D NTT layout
-	int LA, LB;                          // column levels, row levels
+	u32 R, H;                            // column pass: row length and row count of the 2-D layout
+	u32 HR;                              // row pass: rows (H 2^G) of 2^(LB+1) words
+	int LA, LB, G;                       // column levels, row levels, mid levels (lengths above 2^20)
 };
 
 // Digit size of one candidate (candidates of a batch share K and the length).

@@ -320,7 +320,8 @@ struct ab_transform
 		const size_t n = (size_t)1 << prm.ln;
 		std::memset(&tc, 0, sizeof(tc));
 		tc.K = K; tc.KP = KP; tc.pck = prm.pck; tc.lbase = prm.lbase; tc.ln = prm.ln;
-		tc.n = (u32)n; tc.R = geo.R; tc.H = geo.H; tc.LA = geo.LA; tc.LB = geo.LB;
+		tc.n = (u32)n;
+		apply_geometry(tc, geo);
 		mpz_t M, Mk, t, mod; mpz_inits(M, Mk, t, mod, nullptr);
 		mpz_set_ui(M, 1);
 		for (int k = 0; k < KP; ++k) mpz_mul_ui(M, M, TPRIMES[k]);
@@ -435,12 +436,16 @@ struct ab_transform
 	{
 		if (prof_used < prof.size()) CK(cudaEventRecord(prof[prof_used++], st));
 	}
+	// a row pass, with the mid levels before and after it above 2^20
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr, cudaStream_t s = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		const int nj = j1 ? 2 : 1;
 		if (s == nullptr) { mark(); s = st; }
-		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, s));
+		if (geo.G > 0) { CK(launch_midpass(geo, tc, js, nj, s, 1, false)); ++launches; }
+		CK(launch_rowpass(geo, tc, js, nj, s));
 		++launches;
+		if (geo.G > 0 && j0.mode != ROW_FWD_ONLY) { CK(launch_midpass(geo, tc, js, nj, s, 1, true)); ++launches; }
 	}
 	void cols(const ColJob & j0, const ColJob * j1 = nullptr, cudaStream_t s = nullptr)
 	{
@@ -598,7 +603,7 @@ struct ab_transform
 	void use_geometry(const Geometry & g)
 	{
 		geo = g;
-		tc.R = g.R; tc.H = g.H; tc.LA = g.LA; tc.LB = g.LB;
+		apply_geometry(tc, g);
 	}
 
 	// row/column split of the transform (the register layouts do not depend on it)
@@ -690,7 +695,7 @@ struct ab_transform
 		if (prm.K < 2 || prm.K > 5 || (size_t)prm.pck != get_s((size_t)prm.K) || prm.lbase < 2 || prm.lbase > 31 ||
 		    prm.pck * prm.lbase > 80)
 			throw ab_error(AB_E_ARG, "invalid transform parameters");
-		if (!make_geometry(prm.ln, 0, geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length 2^" + std::to_string(prm.ln) + " is not supported (6 <= ln <= 20)");
+		if (!make_geometry(prm.ln, 0, geo)) throw ab_error(AB_E_UNSUPPORTED, "NTT length 2^" + std::to_string(prm.ln) + " is not supported (6 <= ln <= 22)");
 		n = (size_t)1 << prm.ln;
 		KP = prm.K + 1;
 		mpz_t R, Ninv; mpz_inits(R, Ninv, nullptr);
@@ -804,6 +809,7 @@ struct ab_batch
 	std::vector<ab_transform *> views;
 	cudaGraphExec_t gexec = nullptr;
 	int g_steps = 0;
+	uint64_t g_kernels = 0;
 	int zl = 0;                        // slots the graph launches (grid.z): a power of two covering every live slot
 	uint64_t launches = 0;
 
@@ -827,15 +833,21 @@ struct ab_batch
 		return reinterpret_cast<const uint2 *>(base[ab_transform::WC]) + ((q ? 2 : 0) + (inverse ? 1 : 0)) * (cls.K + 1) * COLTW;
 	}
 
+	uint64_t recorded = 0;              // kernels recorded by rows()/cols() (graph nodes)
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
-		CK(launch_rowpass(geo, tc, js, j1 ? 2 : 1, st, zl));
+		const int nj = j1 ? 2 : 1;
+		if (geo.G > 0) { CK(launch_midpass(geo, tc, js, nj, st, zl, false)); ++recorded; }
+		CK(launch_rowpass(geo, tc, js, nj, st, zl));
+		++recorded;
+		if (geo.G > 0 && j0.mode != ROW_FWD_ONLY) { CK(launch_midpass(geo, tc, js, nj, st, zl, true)); ++recorded; }
 	}
 	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
 	{
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, zl));
+		++recorded;
 	}
 	RowJob rj(u32 * x, int mode, bool q, const u32 * xp, const u32 * act) const
 	{
@@ -1551,6 +1563,7 @@ int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t
 			if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
 			b->zl = zl;
 			cudaGraph_t g = nullptr;
+			b->recorded = 0;
 			CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
 			try { b->record_steps(steps); }
 			catch (...) { cudaStreamEndCapture(b->st, &g); if (g) cudaGraphDestroy(g); throw; }
@@ -1559,9 +1572,10 @@ int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t
 			cudaGraphDestroy(g);
 			CK(e);
 			b->g_steps = steps;
+			b->g_kernels = b->recorded;
 		}
 		CK(cudaGraphLaunch(b->gexec, b->st));
-		b->launches += 1 + 6 * (uint64_t)steps;       // kernels of the graph
+		b->launches += b->g_kernels;                  // kernels of the graph
 		for (ab_transform * v : b->views) if (v) v->prefwd = false;
 	});
 }
@@ -1574,7 +1588,7 @@ int ab_batch_set_geometry(ab_batch * b, int lb)
 		if (!make_geometry(b->cls.ln, lb, g)) throw ab_error(AB_E_ARG, "geometry not available for this length");
 		CK(cudaStreamSynchronize(b->st));
 		b->geo = g;
-		b->tc.R = g.R; b->tc.H = g.H; b->tc.LA = g.LA; b->tc.LB = g.LB;
+		apply_geometry(b->tc, g);
 		for (ab_transform * v : b->views) if (v) { v->use_geometry(g); v->prefwd = false; }
 		RowJobs rjs{}; ColJobs cjs{};
 		CK(launch_rowpass(b->geo, b->tc, rjs, 1, b->st, 0));

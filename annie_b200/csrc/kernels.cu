@@ -231,15 +231,15 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 	const u32 cand = blockIdx.z;
 	if (J.active != nullptr && J.active[cand] == 0u) return;
 	const size_t cofs = (size_t)cand * J.stride;
-	const u32 k = blockIdx.x / c.H, r = blockIdx.x - k * c.H;
+	const u32 k = blockIdx.x / c.HR, r = blockIdx.x - k * c.HR;
 	const u32 p = c.p[k], p2 = 2 * p, pinv = c.pinv[k];
 	u32 * __restrict__ x = J.x + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
 	RowTw tw;
 	tw.w = J.w + (size_t)k * (c.n >> 1);
 	tw.wi = (J.wi != nullptr) ? J.wi + (size_t)k * (c.n >> 1) : nullptr;
-	tw.H = c.H;
+	tw.H = c.HR;
 	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
-	const u32 Hr = c.H + r;
+	const u32 Hr = c.HR + r;
 	const u32 tid = threadIdx.x;
 	u32 v[RP_EPT];
 	// twiddles of the last forward level of virtual thread vt: the c of its polynomials
@@ -817,20 +817,73 @@ __global__ void k_import(const RefConst rc, const u32 * __restrict__ words, u32 
 	for (int l = 0; l < AB_NW; ++l) norm[(size_t)l * n + i] = x[l];
 }
 
+// ================================================================ mid pass
+// The G levels between the column and the row levels (lengths above 2^20):
+// with i = (h 2^G + m) R + c, global level LA + t works on bit G-1-t of m,
+// block j = h 2^t + (m >> (G - t)).  One thread per (prime, h, c): 2^G words
+// at stride R (consecutive threads, consecutive c).  Forward: [0, 4p) in and
+// out; inverse: [0, 2p), twiddles -w^-1 (domain Q: the mirrored w).
+template <int G, bool INV>
+__global__ void __launch_bounds__(256) k_midpass(const RowJobs jobs, const TConst c)
+{
+	constexpr int M = 1 << G;
+	const RowJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
+	const u32 cand = blockIdx.z;
+	if (J.active != nullptr && J.active[cand] == 0u) return;
+	const u32 R = c.R >> G;                      // row-pass row length
+	const u32 per = c.H * R;
+	const u32 gid = blockIdx.x * blockDim.x + threadIdx.x;
+	if (gid >= (u32)c.KP * per) return;
+	const u32 k = gid / per, rem = gid - k * per, h = rem / R, col = rem - h * R;
+	const u32 p = c.p[k], p2 = 2 * p;
+	u32 * __restrict__ x = J.x + (size_t)cand * J.stride + (size_t)k * c.n + (size_t)h * M * R + col;
+	const uint2 * __restrict__ w = J.w + (size_t)k * (c.n >> 1);
+	const uint2 * __restrict__ wi = (J.wi != nullptr) ? J.wi + (size_t)k * (c.n >> 1) : nullptr;
+	u32 v[M];
+#pragma unroll
+	for (int m = 0; m < M; ++m) v[m] = x[(size_t)m * R];
+#pragma unroll
+	for (int tt = 0; tt < G; ++tt)
+	{
+		const int t = INV ? G - 1 - tt : tt;
+		const int half = M >> (t + 1);
+		const u32 lvl = 1u << (c.LA + t);
+#pragma unroll
+		for (int blk = 0; blk < (1 << t); ++blk)
+		{
+			const u32 idx = lvl + (h << t) + (u32)blk;
+			const uint2 wv = !INV ? __ldg(w + idx) : (wi != nullptr) ? __ldg(wi + idx) : __ldg(w + (3u * lvl - 1u - idx));
+#pragma unroll
+			for (int q = 0; q < half; ++q)
+			{
+				const int m0 = blk * 2 * half + q;
+				if (INV) inv_bf(v[m0], v[m0 + half], wv.x, wv.y, p, p2);
+				else fwd_bf(v[m0], v[m0 + half], wv.x, wv.y, p, p2);
+			}
+		}
+	}
+#pragma unroll
+	for (int m = 0; m < M; ++m) x[(size_t)m * R] = v[m];
+}
+
 // ================================================================ host side
 bool make_geometry(int ln, int lb_override, Geometry & g)
 {
-	if (ln < 6 || ln > 20) return false;
+	if (ln < 6 || ln > 22) return false;
 	const int L = ln - 1;
 	// default split, measured on B200 for single transforms (us per squaring
 	// over every split, ln 9..19): the row pass gets L - 2 levels up to 2^12
-	// points, then 11 levels, and the column pass takes the rest (at most 6)
-	static const int DEFAULT_LB[21] = {0, 0, 0, 0, 0, 0, 4, 4, 5, 6, 7, 8, 9, 10, 10, 11, 11, 11, 11, 12, 13};
+	// points, then 11 levels, and the column pass takes the rest (at most 6);
+	// above 2^20 the row and column passes are full (13 and 6 levels) and the
+	// mid pass takes the 1 or 2 levels left
+	static const int DEFAULT_LB[23] = {0, 0, 0, 0, 0, 0, 4, 4, 5, 6, 7, 8, 9, 10, 10, 11, 11, 11, 11, 12, 13, 13, 13};
 	int LB = (lb_override > 0) ? lb_override : DEFAULT_LB[ln];
-	if (lb_override <= 0 && L - LB > 6) LB = L - 6;
-	if (LB < 4 || LB > 13 || LB > L - 1 || L - LB > 6) return false;
-	g.ln = ln; g.LB = LB; g.LA = L - LB;
-	g.H = 1u << g.LA; g.R = 1u << (LB + 1); g.C = CC;
+	if (lb_override <= 0 && L - LB > 6 && ln <= 20) LB = L - 6;
+	if (LB < 4 || LB > 13 || LB > L - 1) return false;
+	const int LA = (L - LB < 6) ? L - LB : 6, G = L - LB - LA;
+	if (G > 3) return false;
+	g.ln = ln; g.LB = LB; g.LA = LA; g.G = G;
+	g.H = 1u << LA; g.R = 1u << (LB + 1); g.HR = g.H << G; g.RC = g.R << G; g.C = CC;
 	return true;
 }
 
@@ -863,7 +916,7 @@ static cudaError_t rowpass_t(const Geometry & g, const TConst & c, const RowJobs
 	const cudaError_t e = allow_dynamic_smem(k_rowpass<LOG_R>, smem, attr_done);
 	if (e != cudaSuccess) return e;
 	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
-	const dim3 grid((unsigned)(c.KP * g.H), (unsigned)njobs, (unsigned)ncand);
+	const dim3 grid((unsigned)(c.KP * g.HR), (unsigned)njobs, (unsigned)ncand);
 	k_rowpass<LOG_R><<<grid, RowCfg<LOG_R>::NT, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }
@@ -886,6 +939,28 @@ cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs &
 	}
 }
 
+template <int G>
+static cudaError_t midpass_t(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand, bool inverse)
+{
+	const u32 threads = (u32)c.KP * g.H * g.R;
+	const dim3 grid((threads + 255) / 256, (unsigned)njobs, (unsigned)ncand);
+	if (inverse) k_midpass<G, true><<<grid, 256, 0, s>>>(jobs, c);
+	else k_midpass<G, false><<<grid, 256, 0, s>>>(jobs, c);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_midpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand, bool inverse)
+{
+	if (ncand == 0) return cudaSuccess;
+	switch (g.G)
+	{
+	case 1: return midpass_t<1>(g, c, jobs, njobs, s, ncand, inverse);
+	case 2: return midpass_t<2>(g, c, jobs, njobs, s, ncand, inverse);
+	case 3: return midpass_t<3>(g, c, jobs, njobs, s, ncand, inverse);
+	default: return cudaErrorInvalidValue;
+	}
+}
+
 template <int LOG_H, int K, int PCK>
 static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand)
 {
@@ -894,7 +969,7 @@ static cudaError_t colpass_t(const Geometry & g, const TConst & c, const ColJobs
 	const cudaError_t e = allow_dynamic_smem(k_colpass<LOG_H, K, PCK>, smem, attr_done);
 	if (e != cudaSuccess) return e;
 	if (ncand == 0) return cudaSuccess;      // set-up only (before a stream capture)
-	const dim3 grid(g.R / CC, (unsigned)njobs, (unsigned)ncand);
+	const dim3 grid(g.RC / CC, (unsigned)njobs, (unsigned)ncand);
 	k_colpass<LOG_H, K, PCK><<<grid, COL_THREADS, smem, s>>>(jobs, c);
 	return cudaGetLastError();
 }

@@ -70,20 +70,33 @@ struct ColJob
 };
 struct ColJobs { ColJob j[2]; };
 
+// Split of the ln - 1 levels: LA column levels, G mid levels, LB row levels.
+// Coefficient i = (h 2^G + m) R + c with h < H = 2^LA rows for the column
+// pass (whose rows are RC = R 2^G words), m < 2^G, and c < R = 2^(LB+1); the
+// row pass sees HR = H 2^G rows of R words.  G > 0 only above 2^20.
 struct Geometry
 {
-	int ln, LA, LB;
-	u32 H, R;
+	int ln, LA, LB, G;
+	u32 H, R, HR, RC;
 	int C;               // columns per column-pass CTA
 };
 
-// Chooses the 2-D split for a transform of length 2^ln (6 <= ln <= 20).
+// Chooses the split for a transform of length 2^ln (6 <= ln <= 22);
+// lb_override > 0 asks for that many row levels.
 bool make_geometry(int ln, int lb_override, Geometry & g);
+
+// The launch constants that describe a split.
+inline void apply_geometry(TConst & c, const Geometry & g)
+{
+	c.R = g.RC; c.H = g.H; c.HR = g.HR; c.LA = g.LA; c.LB = g.LB; c.G = g.G;
+}
 
 // Column-pass scratch in shared memory, bytes.
 size_t colpass_smem(const Geometry & g, int KP);
 
 cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
+// The G mid levels of the row jobs' buffers, forward or inverse (G > 0).
+cudaError_t launch_midpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand, bool inverse);
 cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
 
 // Register words of the reference (K planes of residues mod its primes) from

@@ -144,6 +144,8 @@ int mpz_cmp(mpz_srcptr, mpz_srcptr);
 int mpz_cmp_ui(mpz_srcptr, unsigned long int);
 #define mpz_tstbit __gmpz_tstbit
 int mpz_tstbit(mpz_srcptr, mp_bitcnt_t);
+#define mpz_setbit __gmpz_setbit
+void mpz_setbit(mpz_ptr, mp_bitcnt_t);
 #define mpz_sizeinbase __gmpz_sizeinbase
 size_t mpz_sizeinbase(mpz_srcptr, int);
 #define mpz_size __gmpz_size

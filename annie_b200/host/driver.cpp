@@ -316,9 +316,99 @@ int run(const mpz_t n, const ab_prp_options & o, ab_prp_result & r)
 	std::snprintf(r.message, sizeof(r.message), "Validation failed!");
 	return 1;
 }
+// One size of the reference's benchmark mode annie::bench
+// (src/annie.h:432-556): N = 3 2^e + 1 with base 3; the exponentiation to
+// 6^50 with its Gerbicz-Li products and final check (it must validate), then
+// square_mul with multipliers 3, 1, 3, 1, ... for `seconds` of wall clock.
+// The reference times one square_mul call at a time on a 10 s thread timer;
+// here the squarings run in graph-replayed runs of 4096 and the clock stops
+// after the device has finished (a synchronising copy, as the reference's).
+void bench_one(uint64_t e, int device, double seconds, ab_bench_row & row)
+{
+	using clk = std::chrono::steady_clock;
+	mpz_t n, exponent, res, r1, r2, alt;
+	mpz_inits(n, exponent, res, r1, r2, alt, nullptr);
+	mpz_ui_pow_ui(exponent, 6, 50);
+	const int B = gl_block_size(mpz_sizeinbase(exponent, 2));
+	chunk_sum(res, exponent, B);
+	mpz_set_ui(n, 3); mpz_mul_2exp(n, n, (mp_bitcnt_t)e); mpz_add_ui(n, n, 1);
+	std::memset(&row, 0, sizeof(row));
+	row.e = e;
+	row.digits = (int64_t)mpz_sizeinbase(n, 10);
+	{
+		transformCUDA t(n, 3, device);
+		const ab_params & p = t.params();
+		row.K = p.K; row.pck = p.pck; row.ln = p.ln; row.lbase = p.lbase;
+		if (t.init_failed()) { row.validated = -1; mpz_clears(n, exponent, res, r1, r2, alt, nullptr); return; }
+		t.set1();
+		t.copy(transform::Reg1, transform::Reg0);
+		for (int i = int(mpz_sizeinbase(exponent, 2)) - 1; i >= 0; --i)
+		{
+			t.square_mul(mpz_tstbit(exponent, (mp_bitcnt_t)i) ? 3 : 1);
+			if ((i % B == 0) && (i / B != 0)) t.mul(transform::Reg1, transform::Reg0);
+		}
+		t.copy(transform::Reg2, transform::Reg0);
+		t.mul(transform::Reg2, transform::Reg1);
+		t.square_mul(1);
+		const int rs = int(mpz_sizeinbase(res, 2));
+		t.set1();
+		for (int i = rs - 1; i >= B; --i) t.square_mul(mpz_tstbit(res, (mp_bitcnt_t)i) ? 3 : 1);
+		t.mul(transform::Reg0, transform::Reg1);
+		for (int i = B - 1; i >= 0; --i) t.square_mul(((i < rs) && mpz_tstbit(res, (mp_bitcnt_t)i)) ? 3 : 1);
+		t.get(r1, transform::Reg0);
+		t.get(r2, transform::Reg2);
+		row.validated = (mpz_cmp(r1, r2) == 0) ? 1 : 0;
+		if (row.validated == 1)
+		{
+			// bits 4095, 4093, ... set: multipliers 3, 1, 3, 1, ... from the top
+			const long RUN = 4096;
+			mpz_set_ui(alt, 0);
+			for (long b = RUN - 1; b >= 0; b -= 2) mpz_setbit(alt, (mp_bitcnt_t)b);
+			t.copy(transform::Reg2, transform::Reg0);      // synchronise before the clock starts
+			const auto t0 = clk::now();
+			double dt = 0;
+			int64_t count = 0;
+			while (dt < seconds)
+			{
+				t.square_mul_bits(alt, RUN - 1, RUN, 3);
+				count += RUN;
+				if (ab_synchronize(t.handle()) != AB_OK) throw std::runtime_error(ab_last_error());
+				dt = std::chrono::duration<double>(clk::now() - t0).count();
+			}
+			row.squarings = count;
+			row.ms_per_bit = dt / (double)count * 1e3;
+			row.estimated_seconds = dt / (double)count * (double)mpz_sizeinbase(n, 2);
+		}
+	}
+	mpz_clears(n, exponent, res, r1, r2, alt, nullptr);
+}
 } // namespace
 
 extern "C" {
+
+int ab_bench_table(int device, const uint64_t * e_list, int count, double seconds, ab_bench_row * rows)
+{
+	if (e_list == nullptr || rows == nullptr || count < 0) return -1;
+	int done = 0;
+	try
+	{
+		for (int i = 0; i < count; ++i)
+		{
+			bench_one(e_list[i], device, seconds, rows[i]);
+			++done;
+			// the reference stops at a failed test; a number that shares a factor
+			// with R (3 2^664381 + 1 = 7 x ...) is recorded and skipped: the
+			// reference never checks init_failed() here (src/annie.h:455-465)
+			if (rows[i].validated == 0) break;
+		}
+	}
+	catch (const std::exception & e)
+	{
+		std::fprintf(stderr, "ab_bench_table: %s\n", e.what());
+		return -1;
+	}
+	return done;
+}
 
 void ab_prp_options_default(ab_prp_options * o)
 {

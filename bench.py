@@ -408,9 +408,10 @@ def run_batch_workload(args, world=1, rank=0, local=0, pg=None):
         t_plain += squarings / single_rate
         per_class.append({"class": list(cls), "candidates": len(members), "row_levels": lb,
                           "batched_sq_per_s": round(batch_rate, 1), "single_us_per_sq": round(1e6 / single_rate, 2)})
-    # (with several ranks, the plain path runs one test per GPU at a time)
-    micro = world * len(cands) / (t_batch / 3600.0)
-    plain = world * len(cands) / (t_plain / 3600.0)
+    # (with several ranks, the plain path runs one test per GPU at a time);
+    # rates in full tests per hour: the candidates that need the exponentiation
+    micro = world * full / (t_batch / 3600.0)
+    plain = world * full / (t_plain / 3600.0)
 
     # the runner on the whole candidate list: admission by size class and HBM
     # budget, autotuned split per class, graph-captured chunks, Gerbicz-Li
@@ -440,21 +441,21 @@ def run_batch_workload(args, world=1, rank=0, local=0, pg=None):
     # candidates decided at set-up take no squaring: the list's time is the
     # squarings of the others at the runner's rate
     total_need = sum(need(k, n) for m in classes.values() for k, n, _ in m)
-    value = len(cands) * 3600.0 * rate / total_need
-    return {"metric": "proth_candidates_per_hour_batched", "value": round(value, 3), "unit": "candidates/hour",
+    value = full * 3600.0 * rate / total_need
+    return {"metric": "proth_full_tests_per_hour_batched", "value": round(value, 3), "unit": "full tests/hour",
             "n_gpus": 1, "steps": 1, "warmup": 2, "ms_per_step": round(window * 1e3, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Proth candidates)",
             "config": {"workload": "4096 Proth k*2^n+1, k odd in [3,2^20), n in [500000,3000000] (xoshiro256** seed 2024), Euler",
                        "slots_per_class": CAP, "squarings_per_graph": S, "hbm_budget_gb": args.batch_hbm_gb,
                        "method": "continuous-batching runner over all 4096 candidates: squarings completed in a %.0f s "
-                                 "window after admission; the list's time = iterations the %d candidates without a factor "
-                                 "in common with R need / that rate (the other %d are decided at set-up by the gcd)"
-                                 % (args.batch_window, full, len(cands) - full)},
+                                 "window after admission; full tests per hour = the %d candidates without a factor in "
+                                 "common with R over (the iterations they need / that rate); the other %d are decided "
+                                 "at set-up by the gcd and are not counted" % (args.batch_window, full, len(cands) - full)},
             "runner": {"in_flight": active, "queued": queued, "batches": st["batches"], "admission_s": round(admit_s, 2),
                        "squarings_per_s": round(rate, 1), "decided_or_finished_in_window": done,
-                       "full_tests_per_hour": round(full * 3600.0 * rate / total_need, 3)},
-            "plain_candidates_per_hour": round(plain, 3), "speedup_vs_plain": round(value / plain, 3),
-            "microbench_candidates_per_hour": round(micro, 3),
+                       "candidates_per_hour_incl_gcd_decided": round(len(cands) * 3600.0 * rate / total_need, 3)},
+            "plain_full_tests_per_hour": round(plain, 3), "speedup_vs_plain": round(value / plain, 3),
+            "microbench_full_tests_per_hour": round(micro, 3),
             "classes": per_class}
 
 
@@ -677,6 +678,77 @@ def run_proth2m_workload(args):
                                        "check, the reload of the verified state and the repeated, verified block"}}
 
 
+def run_table_workload(args):
+    """The reference's own benchmark table (annie::bench, src/annie.h:432-556):
+    N = 3 2^e + 1 for its 13 exponents (33,216 to 159,200,000 bits), each a
+    Gerbicz-Li-validated exponentiation to 6^50, then squarings for a fixed
+    time; ms per bit and the estimated time of a full test."""
+    import annie_b200 as A
+    rows = A.bench_table(seconds=args.table_seconds)
+    out = [{"N": "3*2^%d+1" % r["e"], "digits": r["digits"], "K": r["K"], "pck": r["pck"], "ln": r["ln"], "lbase": r["lbase"],
+            "validated": {1: True, 0: False, -1: "N shares a factor with R (init_failed)"}[r["validated"]],
+            "ms_per_bit": round(r["ms_per_bit"], 5),
+            "estimated_test_hours": round(r["estimated_seconds"] / 3600, 3), "squarings_timed": r["squarings"]} for r in rows]
+    head = [r for r in out if r["N"] == "3*2^33219278+1"]
+    return {"metric": "ms_per_bit_3x2^33219278+1", "value": head[0]["ms_per_bit"] if head else None, "unit": "ms/bit",
+            "n_gpus": 1, "steps": len(out), "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic (the reference's benchmark numbers 3*2^e+1)",
+            "config": {"workload": "annie -h benchmark table: 3*2^e+1, base 3, e in %s" % A.BENCH_TABLE_E,
+                       "seconds_per_size": args.table_seconds},
+            "all_validated": all(r["validated"] is not False for r in out) and len(out) == len(A.BENCH_TABLE_E), "rows": out}
+
+
+def side_proth2m(args):
+    """C2 as a sub-object of the default line, with its own parity window."""
+    r = run_proth2m_workload(args)
+    out = {"us_per_iteration": r["value"], "iterations_timed": args.proth_squarings, "ms_per_gl_block": r["ms_per_step"],
+           "gl_block": r["config"]["gl_block"], "params": {"K": r["config"]["K"], "ln": r["config"]["ln"], "lbase": r["config"]["lbase"]},
+           "workload": r["config"]["workload"], "gl_check": r["gl_check"], "injected_error": r["injected_error"]}
+    if not args.no_cpu_baseline:
+        out["parity"] = proth2m_parity(args)
+    return out
+
+
+def proth2m_parity(args, count=64):
+    """Registers after `count` Euler-test iterations from set1 and Reg1 *= Reg0,
+    against the reference's transformCPU on the same N (checker leg)."""
+    import annie_b200 as A
+    from annie_b200.synth import proth_2m
+    k, N, a = proth_2m(args.proth_n, 11, usable=lambda N, a: not A.probe(N, a)[1])
+    E = (N - 1) >> 1
+    top = E.bit_length() - 1
+    mults = [a if (E >> (top - i)) & 1 else 1 for i in range(count)]
+    t = A.Transform(N, a)
+    t.set1()
+    t.copy(1, 0)
+    for m in mults:
+        t.square_mul(m)
+    t.mul(1, 0)
+    regs = np.concatenate([t.read_register(0), t.read_register(1)])
+    t.close()
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import cpu_baseline
+        ref = cpu_baseline.reference_registers(N, a, mults)
+    except RuntimeError as e:
+        return {"checked": False, "equal": None, "why": str(e)}
+    rec = parity_record(regs, {"regs": ref})
+    rec["window"] = "Reg0 = 1, Reg1 = Reg0, %d Euler-test iterations from the top bit of E = (N - 1)/2, then Reg1 *= Reg0" % count
+    return rec
+
+
+def side_batch(args):
+    """C4 as a sub-object of the default line (a shorter runner window)."""
+    import copy
+    a2 = copy.copy(args)
+    a2.batch_window = args.side_batch_window
+    r = run_batch_workload(a2)
+    return {"full_tests_per_hour": r["value"], "plain_full_tests_per_hour": r["plain_full_tests_per_hour"],
+            "speedup_vs_plain": r["speedup_vs_plain"], "microbench_full_tests_per_hour": r["microbench_full_tests_per_hour"],
+            "runner_squarings_per_s": r["runner"]["squarings_per_s"], "window_s": a2.batch_window,
+            "size_classes": len(r["classes"]), "workload": r["config"]["workload"], "method": r["config"]["method"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -687,7 +759,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="square33M", choices=["square33M", "proth2M", "batch", "serve"])
+    ap.add_argument("--workload", default="square33M", choices=["square33M", "proth2M", "batch", "serve", "table"])
+    ap.add_argument("--table-seconds", type=float, default=10.0)
     ap.add_argument("--batch-slots", type=int, default=64)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.1, 0.4])
     ap.add_argument("--serve-bits", type=int, nargs=2, default=[100000, 400000])
@@ -696,6 +769,9 @@ def main():
     ap.add_argument("--proth-n", type=int, default=2000000)
     ap.add_argument("--batch-window", type=float, default=30.0)
     ap.add_argument("--batch-hbm-gb", type=int, default=16)
+    ap.add_argument("--no-side-workloads", action="store_true",
+                    help="default run: skip the Proth n=2M and 4096-candidate batch sub-objects")
+    ap.add_argument("--side-batch-window", type=float, default=15.0)
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.workload == "batch":
@@ -710,7 +786,7 @@ def main():
     if args.workload != "square33M":
         # single-test latency workloads: one GPU (rank 0); other ranks have no work
         if rank == 0:
-            fn = {"proth2M": run_proth2m_workload, "serve": run_serve_workload}[args.workload]
+            fn = {"proth2M": run_proth2m_workload, "serve": run_serve_workload, "table": run_table_workload}[args.workload]
             print(json.dumps(fn(args)), flush=True)
         if pg is not None:
             pg.destroy_process_group()
@@ -744,6 +820,11 @@ def main():
                       "iterations) at 33.2M bits, set-up untimed; one core: %.0f us/squaring"
                       % (res["cores"], PARITY_WINDOW, res["single_us"])}
     line["parity"] = parity_record(regs, res)
+    if world == 1 and not args.no_side_workloads:
+        # the other configurations the driver should see measured: the Proth
+        # n = 2,000,000 test (C2) and the 4096-candidate batch (C4)
+        line["proth2M"] = side_proth2m(args)
+        line["batch"] = side_batch(args)
     print(json.dumps(line), flush=True)
     if line["parity"]["checked"] and not line["parity"]["equal"]:
         sys.stderr.write("PARITY FAILURE: registers differ from the reference after the window\n")

@@ -52,6 +52,28 @@ int ab_prp_check(const uint64_t * N, size_t nlimbs, const ab_prp_options * opt, 
 void ab_prp_quit(void);
 void ab_prp_reset_quit(void);
 
+/* One row of the benchmark table of the reference's -h mode (annie::bench,
+   src/annie.h:432-556): N = 3 2^e + 1, base 3. */
+typedef struct
+{
+	uint64_t e;
+	int64_t digits;            /* decimal digits of N (mpz_sizeinbase(N, 10), as printed by the reference) */
+	int K, pck, ln, lbase;
+	int validated;             /* 1: the Gerbicz-Li check of the 6^50 exponentiation held; 0: test failed; -1: init failed */
+	int64_t squarings;         /* timed square_mul calls */
+	double ms_per_bit;         /* milliseconds per square_mul (one bit of the exponent) */
+	double estimated_seconds;  /* ms_per_bit x bits of N: the time of a full test */
+} ab_bench_row;
+
+/* The reference's benchmark mode (annie::bench, src/annie.h:432-556) over the
+   exponents e_list[0..count): for each, a Gerbicz-Li-validated exponentiation
+   to 6^50 on a fresh transform, then `seconds` of squarings (the reference
+   uses 10).  Stops after a row that does not validate, as the reference does;
+   a row whose N shares a factor with the transform's R (validated = -1) is
+   recorded and the table goes on.  Returns the rows written, or -1 on an
+   error. */
+int ab_bench_table(int device, const uint64_t * e_list, int count, double seconds, ab_bench_row * rows);
+
 #ifdef __cplusplus
 }
 #endif

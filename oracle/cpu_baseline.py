@@ -56,6 +56,40 @@ def _worker(args):
     return dt, regs
 
 
+def _registers_worker(args):
+    limbs, a, mults = args
+    sys.path.insert(0, HERE)
+    import tempfile
+    import pyoracle
+    N = int.from_bytes(bytes(limbs), "little")
+    t = pyoracle.RefTransform(N, a, 0)
+    t.set1()
+    t.copy(1, 0)
+    t.square_mul_seq(mults)
+    t.mul(1, 0)
+    fd, path = tempfile.mkstemp()
+    os.close(fd)
+    try:
+        return t.checkpoint_words(path)
+    finally:
+        os.unlink(path)
+        t.close()
+
+
+def reference_registers(N, a, mults):
+    """Reg0 || Reg1 of the reference's transformCPU after set1, Reg1 = Reg0, the
+    square_mul calls with multipliers `mults`, and Reg1 *= Reg0 (in a spawned
+    process)."""
+    import pyoracle
+    if not pyoracle.ref_available():
+        pyoracle.build()
+    if not pyoracle.ref_available():
+        raise RuntimeError("the reference's transformCPU is not built (oracle/_ref/libannie_ref.so)")
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.map(_registers_worker, [(list(N.to_bytes((N.bit_length() + 7) // 8, "little")), a, list(mults))])[0]
+
+
 def run(bits, seed, a=3, squarings=2, procs=None):
     """Returns dict(value_us=aggregate microseconds per squaring, single_us=one
     core's microseconds per squaring, cores=P, squarings=total, seconds=the

@@ -107,6 +107,9 @@ def lib_ref():
         L.ref_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_cpu_get_n_base.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_double, C.c_double]
         L.ref_check.argtypes = [_u64p, C.c_size_t, C.c_int, C.c_int, C.c_char_p]
+        L.ref_file_write_checkpoint.argtypes = [C.c_char_p, C.c_int, C.c_double, C.POINTER(C.c_uint8), C.c_size_t]
+        L.ref_file_read_checkpoint.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                               C.POINTER(C.c_uint8), C.c_size_t]
         _lib_ref = L
     return _lib_ref
 
@@ -283,7 +286,28 @@ class RefTransform:
         assert cnt >= 0
         return limbs_to_int(out, cnt)
 
+    def load_checkpoint_words(self, words, path):
+        """Reg0 || Reg1 (plane-major, K*n words each) through the reference's own
+        read_checkpoint (format of src/transformCPU.h:1475-1491)."""
+        np.ascontiguousarray(words, dtype=np.uint32).tofile(path)
+        assert self.L.ref_read_checkpoint(self.h, path.encode()) == 0
+
     def checkpoint_words(self, path):
         """Reg0 and Reg1 as saved by the reference (plane-major, K*n words each)."""
         assert self.L.ref_save_checkpoint(self.h, path.encode()) == 0
         return np.fromfile(path, dtype=np.uint32)
+
+
+def ref_file_write_checkpoint(path, i, elapsed, payload):
+    """A checkpoint file written by the reference's file class (src/file.h) in the
+    layout of annie::save_checkpoint (src/annie.h:162-181)."""
+    buf = np.frombuffer(payload, dtype=np.uint8).copy()
+    return lib_ref().ref_file_write_checkpoint(path.encode(), i, elapsed, buf.ctypes.data_as(C.POINTER(C.c_uint8)), len(buf))
+
+
+def ref_file_read_checkpoint(path, size):
+    """(status, i, elapsed, payload bytes) read and seal-checked by the reference's file class."""
+    buf = np.zeros(size, dtype=np.uint8)
+    i, el = C.c_int(), C.c_double()
+    st = lib_ref().ref_file_read_checkpoint(path.encode(), C.byref(i), C.byref(el), buf.ctypes.data_as(C.POINTER(C.c_uint8)), size)
+    return st, i.value, el.value, buf.tobytes()

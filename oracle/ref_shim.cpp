@@ -127,6 +127,35 @@ int ref_read_checkpoint(void * h, const char * path)
 	return t->read_checkpoint(f) ? 0 : -2;
 }
 
+/* Checkpoint files through the reference's own file class (src/file.h), in the
+   layout of annie::save_checkpoint / _read_checkpoint (src/annie.h:140-181):
+   int version = 1, int i, double elapsed, the transform payload, CRC-32 seal.
+   write: 0 or -1.  read: 0, or -1 (no file), -2 (bad header or seal). */
+int ref_file_write_checkpoint(const char * path, int i, double elapsed, const uint8_t * payload, size_t size)
+{
+	file f(path, "wb", false);
+	if (!f.exists()) return -1;
+	const int version = 1;
+	if (!f.write(reinterpret_cast<const char *>(&version), sizeof(version))) return -1;
+	if (!f.write(reinterpret_cast<const char *>(&i), sizeof(i))) return -1;
+	if (!f.write(reinterpret_cast<const char *>(&elapsed), sizeof(elapsed))) return -1;
+	if (!f.write(reinterpret_cast<const char *>(payload), size)) return -1;
+	f.write_crc32();
+	return 0;
+}
+
+int ref_file_read_checkpoint(const char * path, int * i, double * elapsed, uint8_t * payload, size_t size)
+{
+	file f(path);
+	if (!f.exists()) return -1;
+	int version = 0;
+	if (!f.read(reinterpret_cast<char *>(&version), sizeof(version)) || version != 1) return -2;
+	if (!f.read(reinterpret_cast<char *>(i), sizeof(*i))) return -2;
+	if (!f.read(reinterpret_cast<char *>(elapsed), sizeof(*elapsed))) return -2;
+	if (!f.read(reinterpret_cast<char *>(payload), size)) return -2;
+	return f.check_crc32() ? 0 : -2;
+}
+
 /* The reference's own parameter rule for transformCPU (src/transformCPU.h:1493-1515). */
 void ref_cpu_get_n_base(int * ln, int * lbase, int pck, double log2_16aN, double log2_p_2a)
 {

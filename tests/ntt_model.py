@@ -29,29 +29,45 @@ def shoup_const(w, p):
     return (w << 32) // p
 
 
+def _bitrev_array(s):
+    """bitrev(j, s) for j < s (s a power of two)."""
+    j = np.arange(s, dtype=np.int64)
+    r = np.zeros(s, dtype=np.int64)
+    b = s.bit_length() - 1
+    for i in range(b):
+        r |= ((j >> i) & 1) << (b - 1 - i)
+    return r
+
+
+def _powers(x, s, p):
+    """x^j mod p for j < s (numpy, p < 2^30)."""
+    out = np.ones(s, dtype=np.uint64)
+    j = np.arange(s, dtype=np.int64)
+    sq = np.uint64(x % p)
+    for i in range(max(1, s.bit_length())):
+        sel = ((j >> i) & 1) == 1
+        out[sel] = out[sel] * sq % np.uint64(p)
+        sq = sq * sq % np.uint64(p)
+    return out
+
+
 def tables(ln, k, domain_q):
     """(w, ws), and for domain R (wi, wis) = -w^-1, at positions s + bitrev(j, s)."""
     p, g = TPRIMES[k], TGEN[k]
     n = 1 << ln
-    w = [0] * (n // 2)
-    wi = [0] * (n // 2)
+    w = np.zeros(n // 2, dtype=np.uint64)
+    wi = np.zeros(n // 2, dtype=np.uint64)
     lvl = ln - 1
     s = n // 4
     while s >= 1:
         rho = pow(g, (p - 1) >> lvl, p)
         rhoi = pow(rho, p - 2, p)
-        t = pow(g, (p - 1) >> (lvl + 1), p) if domain_q else 1
-        ti = 1
-        for j in range(s):
-            jr = bitrev(j, s)
-            w[s + jr] = t
-            wi[s + jr] = (p - ti) % p
-            t = t * rho % p
-            ti = ti * rhoi % p
+        t0 = pow(g, (p - 1) >> (lvl + 1), p) if domain_q else 1
+        pos = s + _bitrev_array(s)
+        w[pos] = _powers(rho, s, p) * np.uint64(t0) % np.uint64(p)
+        wi[pos] = (np.uint64(p) - _powers(rhoi, s, p)) % np.uint64(p)
         s //= 2
         lvl -= 1
-    w = np.array(w, dtype=np.uint64)
-    wi = np.array(wi, dtype=np.uint64)
     ws = (w << np.uint64(32)) // np.uint64(p)
     wis = (wi << np.uint64(32)) // np.uint64(p)
     if domain_q:
@@ -83,13 +99,20 @@ def red2(x, p):
     return np.minimum(x, y)
 
 
-def encode(exact, k):
-    """Residues in [0, 3p) of exact values (python ints, |v| < 2^95), as the column pass."""
-    p = TPRIMES[k]
+def exact_limbs(exact):
+    """Three 32-bit limbs (two's complement, 96 bits) of python-int exact values."""
     d = [int(v) & ((1 << 96) - 1) for v in exact]
     d0 = np.array([x & M32 for x in d], dtype=np.uint64)
     d1 = np.array([(x >> 32) & M32 for x in d], dtype=np.uint64)
-    d2u = np.array([((x >> 64) & M32) ^ 0x80000000 for x in d], dtype=np.uint64)
+    d2 = np.array([(x >> 64) & M32 for x in d], dtype=np.uint64)
+    return d0, d1, d2
+
+
+def encode(exact, k, limbs=None):
+    """Residues in [0, 3p) of exact values (python ints, |v| < 2^95), as the column pass."""
+    p = TPRIMES[k]
+    d0, d1, d2 = exact_limbs(exact) if limbs is None else limbs
+    d2u = d2 ^ np.uint64(0x80000000)
     one_s = (1 << 32) // p
     a = _u(d0 - ((d0 * np.uint64(one_s)) >> np.uint64(32)) * np.uint64(p))
     c32 = (1 << 32) % p

@@ -130,3 +130,15 @@ def test_checkpoint_abort_and_resume(tmp_path):
     assert res["resumed"] == 1 and res["status"] == 0
     assert res["res64"] == ref["res64"] and res["is_prp"] == ref["is_prp"]
     assert not os.path.exists(path)      # cleared on completion (annie.h:428)
+
+
+def test_bench_table_rows_validate():
+    # the reference's -h mode (src/annie.h:432-556) on its first sizes: the
+    # Gerbicz-Li check of the 6^50 exponentiation holds on each transform
+    rows = A.bench_table(A.BENCH_TABLE_E[:4], seconds=0.2)
+    assert len(rows) == 4
+    for r in rows:
+        assert r["validated"] == 1, r
+        assert r["squarings"] > 0 and r["ms_per_bit"] > 0
+        N = 3 * (1 << r["e"]) + 1
+        assert (r["K"], r["pck"], r["ln"], r["lbase"]) == A.probe(N, 3)[0]

@@ -22,11 +22,27 @@ pytestmark = pytest.mark.gpu
 KERNEL_CASES = [
     (5, 6, 18), (5, 8, 18), (5, 10, 18), (5, 12, 18), (5, 13, 17), (5, 15, 17),
     (4, 11, 28), (4, 16, 27), (3, 9, 21), (2, 10, 14), (5, 19, 17), (5, 20, 16),
+    (5, 21, 16),                              # with the mid pass (lengths above 2^20)
 ]
+# the forward transform (against the numpy model) also at the top length
+FORWARD_CASES = KERNEL_CASES + [(5, 22, 16), (4, 22, 25)]
 
 
 def _pck(K):
     return {2: 1, 3: 2, 4: 2, 5: 4}[K]
+
+
+def _transform(K, ln, lbase, seed=11):
+    """An engine transform with forced parameters (N drawn as in _pair)."""
+    params = (K, _pck(K), ln, lbase)
+    bits = max(64, (_pck(K) * lbase << ln) // 2)
+    from annie_b200.synth import Xoshiro256ss
+    rng = Xoshiro256ss(seed)
+    for _ in range(100):
+        cand = rng.random_odd(bits)
+        if not A.probe(cand, 3, forced=params)[1]:
+            return A.Transform(cand, 3, params=params)
+    raise AssertionError("no N")
 
 
 def _pair(oracle_mod, K, ln, lbase, seed=11):
@@ -45,21 +61,22 @@ def _pair(oracle_mod, K, ln, lbase, seed=11):
     return A.Transform(N, 3, params=params), oracle_mod.Oracle(N, 3, params=params)
 
 
-@pytest.mark.parametrize("K,ln,lbase", KERNEL_CASES)
-def test_forward_ntt(oracle_mod, K, ln, lbase):
+@pytest.mark.parametrize("K,ln,lbase", FORWARD_CASES)
+def test_forward_ntt(K, ln, lbase):
     # the engine's own transform (K+1 primes below 2^30, lazily reduced words)
     # against its model, modulo each prime (the lazy representatives depend on
     # which product form a level uses); the reference's transform is checked
     # through the products below
     import ntt_model
-    t, o = _pair(oracle_mod, K, ln, lbase)
+    t = _transform(K, ln, lbase)
     x, exact = random_digits_register(K, _pck(K), ln, lbase, seed=ln * 7 + K, with_exact=True)
     n = 1 << ln
+    limbs = ntt_model.exact_limbs(exact)
     for dom in (0, 1):
         got = t.diag_forward(x, dom)
         for k in range(K + 1):
             pk = ntt_model.TPRIMES[k]
-            exp = ntt_model.forward(ntt_model.encode(exact, k), ln, k, dom == 1, reduce_out=True) % pk
+            exp = ntt_model.forward(ntt_model.encode(exact, k, limbs), ln, k, dom == 1, reduce_out=True) % pk
             g = got[k * n:(k + 1) * n].astype(np.uint64)
             assert np.all(g < 2 * pk), "forward NTT words outside [0, 2p)"
             g %= pk
@@ -188,15 +205,17 @@ def test_graph_runs_equal_single_steps(oracle_mod, K, ln, lbase):
 
 @pytest.mark.parametrize("K,ln,lbase", [(5, 13, 17), (4, 16, 27), (5, 19, 17)])
 def test_every_geometry_gives_the_same_registers(oracle_mod, K, ln, lbase):
+    # every row/column split, and the splits that leave 1 to 3 levels to the
+    # mid pass (the lengths above 2^20 use it)
     t, o = _pair(oracle_mod, K, ln, lbase, seed=4)
     L = ln - 1
-    splits = [lb for lb in range(4, 14) if lb <= L - 1 and L - lb <= 6]
+    splits = [lb for lb in range(4, 14) if lb <= L - 1 and L - lb <= 9]
     assert len(splits) >= 1
     t.set1(); o.set1()
     t.copy(1, 0); o.copy(1, 0)
     for lb in splits:
         t.set_geometry(lb)
-        assert t.geometry() == (lb, L - lb)
+        assert t.geometry() == (lb, min(6, L - lb))
         for a in (3, 1):
             t.square_mul(a); o.square_mul(a)
         t.mul(1, 0); o.mul(1, 0)
@@ -204,3 +223,13 @@ def test_every_geometry_gives_the_same_registers(oracle_mod, K, ln, lbase):
         assert np.array_equal(t.read_register(1), o.read_reg(1)), "Reg1 differs with %d row levels" % lb
     with pytest.raises(RuntimeError):
         t.set_geometry(L + 5)
+
+
+def test_register_words_at_2_22(oracle_mod):
+    # the top length (column, mid and row passes: 6 + 2 + 13 levels) against
+    # the oracle: register words after a square_mul
+    t, o = _pair(oracle_mod, 5, 22, 16, seed=6)
+    assert t.geometry() == (13, 6)
+    t.set1(); o.set1()
+    t.square_mul(3); o.square_mul(3)
+    assert np.array_equal(t.read_register(0), o.read_reg(0))
