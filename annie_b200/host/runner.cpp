@@ -8,6 +8,12 @@
 //   GL_HI   Reg0 = 1, square_mul over the bits of res above B;
 //   GL_LO   Reg0 *= d, then B square_mul with the low bits of res;
 //   check   Reg0 ?= d(t+1) (kept in Reg2).
+// With gl_check_blocks > 0, MAIN stops every gl_check_blocks blocks for a
+// periodic check (not in the reference, which checks only at the end):
+//   CHK_HI, CHK_LO   the same power a^C d_prev^(2^B) with C the chunk sum of
+//                    E >> i, then Reg0 ?= d(t); the test's (Reg0, Reg1) were
+//                    saved before and are restored after; on a mismatch the
+//                    test rolls back to its last verified state.
 // Squarings of all admitted tests run together, one graph launch per chunk
 // and size class; the host steps between phases use the slot's transform.
 #include <algorithm>
@@ -56,12 +62,12 @@ void ck(int rc)
 	if (rc != AB_OK) throw rt_error(ab_last_error());
 }
 
-enum Phase { MAIN, EULER, GL_HI, GL_LO, DONE };
+enum Phase { MAIN, EULER, GL_HI, GL_LO, CHK_HI, CHK_LO, DONE };
 
 struct Job
 {
 	uint64_t tag = 0;
-	mpz_t N, E, res;
+	mpz_t N, E, res, chk;
 	int euler = 0;
 	int32_t a = 2;
 	int B = 0;
@@ -70,17 +76,27 @@ struct Job
 	ab_prp_result r{};
 	std::vector<uint64_t> limbs;
 
-	Job() { mpz_inits(N, E, res, nullptr); }
-	~Job() { mpz_clears(N, E, res, nullptr); }
+	// periodic Gerbicz-Li checks: blocks since the last verified state, the
+	// bit at which the running check was taken, the verified state (payload of
+	// Reg0 and Reg1) and the bit below which it resumes, the state saved while
+	// a check runs
+	int blocks = 0, fails_in_row = 0;
+	long chk_bit = -1, vi = -1;
+	std::vector<uint8_t> vsnap, stash;
+	bool injected = false;
+
+	Job() { mpz_inits(N, E, res, chk, nullptr); }
+	~Job() { mpz_clears(N, E, res, chk, nullptr); }
 
 	// bit that the next squaring of the current phase uses, and its multiplier
 	uint32_t mult_at(long bit) const
 	{
 		if (ph == MAIN) return mpz_tstbit(E, (mp_bitcnt_t)bit) ? (uint32_t)a : 1u;
 		if (ph == EULER) return 1u;
+		if (ph == CHK_HI || ph == CHK_LO) return mpz_tstbit(chk, (mp_bitcnt_t)bit) ? (uint32_t)a : 1u;
 		return mpz_tstbit(res, (mp_bitcnt_t)bit) ? (uint32_t)a : 1u;   // GL_HI / GL_LO
 	}
-	long low_bit() const { return (ph == GL_HI) ? B : 0; }
+	long low_bit() const { return (ph == GL_HI || ph == CHK_HI) ? B : 0; }
 	long remaining() const { return (ph == DONE) ? 0 : i - low_bit() + 1; }
 };
 
@@ -289,8 +305,65 @@ struct ab_runner
 				j->r.gl_block = j->B;
 				j->i = (long)mpz_sizeinbase(j->E, 2) - 1;
 				j->ph = MAIN;
+				if (o.gl_check_blocks > 0) { j->vsnap = payload(v); j->vi = j->i + 1; }
 			}
 		}
+	}
+
+	static std::vector<uint8_t> payload(ab_transform * v)
+	{
+		std::vector<uint8_t> buf(ab_checkpoint_size(v));
+		size_t w = 0;
+		ck(ab_save_checkpoint(v, buf.data(), buf.size(), &w));
+		return buf;
+	}
+
+	// a periodic check at the block boundary just passed (bit chk_bit): Reg2 =
+	// d before this block's factor, Reg1 = d now; save (Reg0, Reg1), then
+	// compute a^C Reg2^(2^B) in Reg0 over the CHK phases
+	void start_check(ab_transform * v, Job * j)
+	{
+		j->stash = payload(v);
+		mpz_t e; mpz_init(e);
+		mpz_fdiv_q_2exp(e, j->E, (mp_bitcnt_t)j->chk_bit);
+		chunk_sum(j->chk, e, j->B);
+		mpz_clear(e);
+		ck(ab_set1(v));
+		++j->r.gl_checks;
+		j->ph = CHK_HI;
+		j->i = (long)mpz_sizeinbase(j->chk, 2) - 1;
+		if (j->i < j->B) { ck(ab_mul(v, 0, 2)); j->ph = CHK_LO; j->i = j->B - 1; }
+	}
+
+	// the check's power is in Reg0: compare with d(t) in Reg1, then resume at
+	// the checked state or roll back to the last verified one
+	void end_check(ab_transform * v, Job * j, std::vector<uint64_t> & buf)
+	{
+		size_t cnt = 0;
+		mpz_t z0, z1; mpz_inits(z0, z1, nullptr);
+		ck(ab_get(v, 0, buf.data(), buf.size(), &cnt)); mpz_import(z0, cnt, -1, 8, 0, 0, buf.data());
+		ck(ab_get(v, 1, buf.data(), buf.size(), &cnt)); mpz_import(z1, cnt, -1, 8, 0, 0, buf.data());
+		const bool ok = mpz_cmp(z0, z1) == 0;
+		mpz_clears(z0, z1, nullptr);
+		j->blocks = 0;
+		j->ph = MAIN;
+		if (ok)
+		{
+			ck(ab_read_checkpoint(v, j->stash.data(), j->stash.size()));
+			j->vsnap.swap(j->stash);
+			j->vi = j->chk_bit;
+			j->i = j->chk_bit - 1;
+			j->fails_in_row = 0;
+		}
+		else
+		{
+			ck(ab_read_checkpoint(v, j->vsnap.data(), j->vsnap.size()));
+			j->i = j->vi - 1;
+			++j->r.gl_failures;
+			++j->r.rollbacks;
+			++j->fails_in_row;
+		}
+		j->stash.clear();
 	}
 
 	// host steps at the end of a phase (src/annie.h:343-403)
@@ -298,6 +371,8 @@ struct ab_runner
 	{
 		ab_transform * v = ab_batch_slot(c.b, slot);
 		std::vector<uint64_t> buf(j->limbs.size() + 2);
+		if (j->ph == CHK_HI) { ck(ab_mul(v, 0, 2)); j->ph = CHK_LO; j->i = j->B - 1; return; }
+		if (j->ph == CHK_LO) { end_check(v, j, buf); return; }
 		size_t cnt = 0;
 		mpz_t z; mpz_init(z);
 		auto get = [&](size_t reg) {
@@ -355,6 +430,14 @@ struct ab_runner
 		finish(j, ok ? 0 : 1, msg);
 	}
 
+	// a test whose checks keep failing (a persistent fault) ends as failed
+	void fail_repeated(Class & c, int slot, Job * j)
+	{
+		ab_batch_release(c.b, slot);
+		c.slots[slot] = nullptr;
+		finish(j, 1, "Validation failed repeatedly (Gerbicz-Li check).");
+	}
+
 	// queues one chunk of the class (asynchronous); returns false when idle
 	bool launch_class(Class & c)
 	{
@@ -368,7 +451,13 @@ struct ab_runner
 		{
 			Job * j = c.slots[s];
 			if (j == nullptr) continue;
-			const long n = std::min<long>(S, j->remaining());
+			long n = std::min<long>(S, j->remaining());
+			if (j->ph == MAIN && o.gl_check_blocks > 0)
+			{
+				// stop the chunk at the boundary where the next check is due
+				const long next_b = (j->i / j->B) * j->B - (long)(o.gl_check_blocks - 1 - j->blocks) * j->B;
+				if (next_b > 0 && next_b <= j->i) n = std::min<long>(n, j->i - next_b + 1);
+			}
 			count[s] = (int)n;
 			for (long t = 0; t < n; ++t)
 			{
@@ -395,10 +484,33 @@ struct ab_runner
 			if (j == nullptr || count[s] == 0) continue;
 			bool snapped = false;
 			for (int t = 0; t < count[s]; ++t) snapped |= c.snap[(size_t)t * cap + s] != 0;
+			const bool was_main = (j->ph == MAIN);
+			const long last = j->i - count[s] + 1;             // the last bit this chunk processed
+			bool check = false;
+			if (snapped && o.gl_check_blocks > 0 && ++j->blocks >= o.gl_check_blocks && last % j->B == 0 && last > 0)
+			{
+				// d before this block's factor, for the check (a chunk holds at most
+				// one boundary of a check: it stops there)
+				ck(ab_copy(ab_batch_slot(c.b, s), 2, 1));
+				check = true;
+			}
 			if (snapped) ck(ab_batch_gl_mul(c.b, s));
 			j->i -= count[s];
 			j->r.squarings += count[s];
 			squarings += (uint64_t)count[s];
+			if (was_main && !j->injected && o.inject_bit >= 0 && j->tag == o.inject_tag && last <= o.inject_bit)
+			{
+				// host-side fault: one word of Reg0 changes between two launches
+				ck(ab_inject_word(ab_batch_slot(c.b, s), 0, o.inject_word, -1));
+				j->injected = true;
+			}
+			if (check && j->remaining() > 0)
+			{
+				if (j->fails_in_row >= 8) { fail_repeated(c, s, j); continue; }
+				j->chk_bit = last;
+				start_check(ab_batch_slot(c.b, s), j);
+				continue;
+			}
 			if (j->remaining() <= 0) next_phase(c, s, j);
 		}
 	}
@@ -413,6 +525,8 @@ void ab_runner_options_default(ab_runner_options * o)
 	o->max_slots_per_class = 256;
 	o->chunk = 64;
 	o->autotune = 1;
+	o->gl_check_blocks = 0;
+	o->inject_bit = -1;
 }
 
 int ab_runner_create(const ab_runner_options * o, ab_runner ** out)

@@ -70,6 +70,13 @@ typedef struct
 	int max_slots_per_class;
 	int chunk;                 /* squarings per graph launch */
 	int autotune;              /* 1: tune the split of each new size class (ab_batch_autotune) */
+	int gl_check_blocks;       /* verify each test's Gerbicz-Li product every this many blocks of B
+	                              squarings and roll back to the last verified state on a mismatch
+	                              (as ab_prp_check); 0 = only the final check of the reference */
+	uint64_t inject_tag;       /* fault injection for tests: the test with this tag gets one word of
+	                              Reg0 changed (ab_inject_word) once its loop passes bit inject_bit */
+	int64_t inject_bit;        /* -1 = no injection */
+	uint32_t inject_word;
 } ab_runner_options;
 
 void ab_runner_options_default(ab_runner_options * o);

@@ -102,6 +102,33 @@ def test_runner_matches_reference_golden_and_solo():
         assert (solo["res64"], solo["is_prp"]) == (got["res64"], got["is_prp"])
 
 
+def test_runner_periodic_check_detects_and_rolls_back():
+    # every test checked every 2 Gerbicz-Li blocks; one test gets a word of
+    # Reg0 changed mid-run: its next check fails, it rolls back to the last
+    # verified state and still ends with the reference's RES64
+    with open(os.path.join(HERE, "golden", "prp_vectors.json")) as f:
+        vec = [v for v in json.load(f) if not v.get("big")]
+    jobs = {}
+    for tag, v in enumerate(vec):
+        N = random_N(v["bits"], v["seed"]) if v["form"] == "random_odd" else proth_N(v["n"], v["seed"])[1]
+        jobs[tag] = (N, v)
+    victim = max(jobs, key=lambda t: jobs[t][0].bit_length())
+    bits = jobs[victim][0].bit_length()
+    r = A.Runner(chunk=32, max_slots_per_class=8, gl_check_blocks=2, inject_tag=victim, inject_bit=bits // 2, inject_word=777)
+    for tag, (N, v) in jobs.items():
+        r.submit(N, euler=bool(v["euler"]), base=v["base"], tag=tag)
+    res = _run_all(r)
+    assert set(res) == set(jobs)
+    for tag, (N, v) in jobs.items():
+        got = res[tag]
+        assert got["status"] == 0, got["message"]
+        assert got["gl_checks"] > 0
+        if v["res64"] is not None:
+            assert "%016X" % got["res64"] == v["res64"]
+    assert res[victim]["gl_failures"] >= 1 and res[victim]["rollbacks"] >= 1
+    assert all(res[t]["gl_failures"] == 0 for t in jobs if t != victim)
+
+
 def test_runner_continuous_admission_under_budget():
     # room for 2 slots of the class at a time: the rest wait and are admitted as slots free up
     nums = _same_class_numbers((5, 4, 10), 5, 50000, 70000, 3)
