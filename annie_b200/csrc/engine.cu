@@ -258,7 +258,8 @@ struct ab_transform
 	mpz_t N, factor;
 	u32 * dmem = nullptr;
 	u32 * d_flag = nullptr;              // import error flag (device word)
-	bool prefwd = false;     // AQ0/AR0 hold the first forward levels of REG0
+	bool prefwd = false;     // AR0 (and AQ0 unless q_pending) hold the first forward levels of REG0
+	bool q_pending = false;  // AQ0 is still to be computed from REG0, at the head of the Q chain
 	std::vector<u32> host;
 	uint64_t launches = 0;   // kernels launched by this handle
 	std::vector<cudaEvent_t> prof;   // non-empty: record an event before every launch
@@ -490,6 +491,9 @@ struct ab_transform
 
 	// reduceMMGW tail (transformGPU.h:523-538): m' = T_R Ninv mod R, +2,
 	// r' = m' N - T_Q mod Q.  AR1 holds the first forward levels of T_R.
+	// With the Q chain on its own stream, the carry-sub leaves only the R-domain
+	// levels (the next squaring's critical path starts there); the Q chain
+	// starts by computing its own from the new Reg0 (q_pending).
 	void reduce_tail(const u32 * tq, u32 * out, bool want_prefwd, bool join_q = false)
 	{
 		rows(rj(b(AR1), ROW_MUL, false, b(NIR)));
@@ -497,8 +501,10 @@ struct ab_transform
 		rows(rj(b(AQ1), ROW_MUL, true, b(NQ)));
 		if (join_q) CK(cudaStreamWaitEvent(st, ev_q, 0));
 		ColJob j2 = cj_tr(b(AQ1), true, 1, tq, LOWER_Q); j2.out_norm = out;
-		if (want_prefwd) set_fwd(j2, b(AQ0), b(AR0));
+		const bool q_chain = overlap || split;   // the Q chain has launches of its own
+		if (want_prefwd) set_fwd(j2, q_chain ? nullptr : b(AQ0), b(AR0));
 		cols(j2);
+		q_pending = want_prefwd && q_chain;
 	}
 
 	// First product of squareMMGW / mulMMGW (transformGPU.h:540-568):
@@ -508,7 +514,7 @@ struct ab_transform
 	// overlap, the Q chain runs on st2 (T_Q is only needed by the final
 	// carry-sub) and reduce_tail joins it.  A non-null `mult` is a device word
 	// read in place of `a` (graph replays).
-	void first_product(u32 a, const u32 * xq, const u32 * xr, const u32 * mult = nullptr)
+	void first_product(u32 a, const u32 * xq, const u32 * xr, const u32 * mult = nullptr, bool q_from_reg0 = false)
 	{
 		RowJob rq = rj(b(AQ0), xq ? ROW_MUL : ROW_SQUARE, true, xq), rr = rj(b(AR0), xr ? ROW_MUL : ROW_SQUARE, false, xr);
 		ColJob jq = cj_tr(b(AQ0), true, a, nullptr, LOWER_NONE); jq.out_norm = b(TQ); jq.mult = mult;
@@ -517,34 +523,39 @@ struct ab_transform
 		{
 			CK(cudaEventRecord(ev_fork, st));
 			CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+			if (q_from_reg0) { ColJob jf = cj_norm(b(REG0)); set_fwd(jf, b(AQ0), nullptr); cols(jf, nullptr, st2); }
 			rows(rq, nullptr, st2);
 			cols(jq, nullptr, st2);
 			CK(cudaEventRecord(ev_q, st2));
 			rows(rr);
 			cols(jr);
 		}
-		else if (split)
-		{
-			// the launches of the overlapped schedule, in order on one stream
-			rows(rq); cols(jq); rows(rr); cols(jr);
-		}
 		else
 		{
-			rows(rq, &rr);
-			cols(jq, &jr);
+			if (q_from_reg0) { ColJob jf = cj_norm(b(REG0)); set_fwd(jf, b(AQ0), nullptr); cols(jf); }
+			if (split)
+			{
+				// the launches of the overlapped schedule, in order on one stream
+				rows(rq); cols(jq); rows(rr); cols(jr);
+			}
+			else
+			{
+				rows(rq, &rr);
+				cols(jq, &jr);
+			}
 		}
 	}
 
 	void prefwd_reg0()
 	{
-		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(AR0)); cols(j); }
+		if (!prefwd) { ColJob j = cj_norm(b(REG0)); set_fwd(j, b(AQ0), b(AR0)); cols(j); q_pending = false; }
 	}
 
 	// squareMMGW (transformGPU.h:556-568)
 	void square_mul(u32 a)
 	{
 		prefwd_reg0();
-		first_product(a, nullptr, nullptr);
+		first_product(a, nullptr, nullptr, nullptr, q_pending);
 		reduce_tail(b(TQ), b(REG0), true, overlap);
 		prefwd = true;
 	}
@@ -575,7 +586,7 @@ struct ab_transform
 			{
 				for (int s = 0; s < G; ++s)
 				{
-					first_product(1, nullptr, nullptr, d_mult + s);
+					first_product(1, nullptr, nullptr, d_mult + s, overlap);
 					reduce_tail(b(TQ), b(REG0), true, overlap);
 				}
 			}
@@ -587,7 +598,7 @@ struct ab_transform
 			cudaGraphDestroy(g);
 			CK(ei);
 		}
-		prefwd_reg0();
+		prefwd_reg0();                           // AR0 (and AQ0, recomputed by the graph's first step)
 		const int hi = mult_i;
 		CK(cudaEventSynchronize(mult_done[hi]));
 		std::memcpy(h_mult[hi], mults, G * sizeof(u32));
@@ -597,6 +608,7 @@ struct ab_transform
 		CK(cudaGraphLaunch(gexec, st));
 		launches += graph_kernels;
 		prefwd = true;
+		q_pending = overlap;                     // as the graph's last step left it
 	}
 
 	// the split and the launch constants that describe it, always together
