@@ -129,10 +129,16 @@ ABI = [
     ("ab_batch_load", [C.c_void_p, C.c_int, _u64p, C.c_size_t, C.c_int32, C.POINTER(C.c_int)], C.c_int),
     ("ab_batch_load_many", [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(C.c_size_t),
                             C.POINTER(C.c_int32), C.POINTER(C.c_int)], C.c_int),
+    ("ab_batch_prepare", [_u64p, C.c_size_t, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(Params), C.POINTER(C.c_int)], C.c_int),
+    ("ab_prepared_factor", [C.c_void_p, _u64p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    ("ab_prepared_bytes", [C.c_void_p], C.c_size_t),
+    ("ab_prepared_destroy", [C.c_void_p], None),
+    ("ab_batch_install", [C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     ("ab_batch_slot", [C.c_void_p, C.c_int], C.c_void_p),
     ("ab_batch_clone", [C.c_void_p, C.c_int, C.c_int], C.c_int),
     ("ab_batch_release", [C.c_void_p, C.c_int], C.c_int),
     ("ab_batch_steps", [C.c_void_p, C.c_int, _u32p, _u8p], C.c_int),
+    ("ab_batch_ready", [C.c_void_p], C.c_int),
     ("ab_batch_gl_mul", [C.c_void_p, C.c_int], C.c_int),
     ("ab_batch_set_geometry", [C.c_void_p, C.c_int], C.c_int),
     ("ab_batch_autotune", [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)], C.c_int),

@@ -1345,7 +1345,13 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 		b->n = (size_t)1 << cls->ln;
 		b->w_ntt = (size_t)(cls->K + 1) * b->n; b->w_norm = (size_t)AB_NW * b->n;
 		CK(cudaSetDevice(device));
-		CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+		// smaller classes at higher stream priority: their chunks are chains of
+		// short, latency-bound launches, which otherwise queue behind the large
+		// grids of the big classes sharing the GPU
+		int least = 0, greatest = 0;
+		CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+		const int prio = std::min(least, greatest + std::max(0, cls->ln - 12));
+		CK(cudaStreamCreateWithPriority(&b->st, cudaStreamNonBlocking, prio));
 		// the flag word, the per-slot buffers (slot-major within each type), then
 		// the shared buffers: the reference words XW and the twiddle tables
 		size_t total = 64, offs[ab_transform::NBUF];
@@ -1491,6 +1497,72 @@ int ab_batch_load_many(ab_batch * b, int count, const int * slots, const uint64_
 			batch_install(b, slots[i], views[i], pp[i]);
 		}
 	});
+}
+
+struct ab_prepared
+{
+	std::unique_ptr<ab_transform> v;
+	ab_transform::Prepared pp;
+};
+
+int ab_batch_prepare(const uint64_t * Nl, size_t nlimbs, int32_t a, ab_prepared ** out, ab_params * params, int * init_failed)
+{
+	if (out) *out = nullptr;
+	ab_prepared * p = nullptr;
+	const int rc = guarded([&] {
+		if (Nl == nullptr || nlimbs == 0 || a < 1 || out == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		std::vector<std::unique_ptr<ab_transform>> views;
+		std::vector<ab_transform::Prepared> pp;
+		batch_prepare(1, &Nl, &nlimbs, &a, views, pp);
+		p = new ab_prepared();
+		p->v = std::move(views[0]);
+		p->pp = std::move(pp[0]);
+		if (params) *params = p->v->prm;
+		if (init_failed) *init_failed = p->v->failed ? 1 : 0;
+	});
+	if (rc != AB_OK) { delete p; return rc; }
+	*out = p;
+	return AB_OK;
+}
+
+int ab_prepared_factor(const ab_prepared * p, uint64_t * out, size_t cap, size_t * count)
+{
+	return guarded([&] {
+		if (p == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+		if (!p->v->failed) throw ab_error(AB_E_ARG, "gcd(N, R) = 1: no factor");
+		const mpz_srcptr z = p->v->factor;
+		const size_t sz = mpz_size(z);
+		if (sz > cap) throw ab_error(AB_E_CAPACITY, "output too small");
+		for (size_t i = 0; i < sz; ++i) out[i] = mpz_getlimbn(z, (mp_size_t)i);
+		*count = sz;
+	});
+}
+
+size_t ab_prepared_bytes(const ab_prepared * p)
+{
+	if (p == nullptr) return 0;
+	return (p->pp.wN.size() + p->pp.wNinv.size() + p->pp.wOne.size()) * sizeof(u32);
+}
+
+void ab_prepared_destroy(ab_prepared * p) { delete p; }
+
+int ab_batch_install(ab_batch * b, int slot, ab_prepared * p)
+{
+	std::unique_ptr<ab_prepared> own(p);
+	return guarded([&] {
+		if (b == nullptr || p == nullptr || slot < 0 || slot >= b->cap) throw ab_error(AB_E_ARG, "bad arguments");
+		batch_install(b, slot, own->v, own->pp);
+	});
+}
+
+int ab_batch_ready(const ab_batch * b)
+{
+	if (b == nullptr) return AB_E_ARG;
+	const cudaError_t e = cudaEventQuery(b->ctrl_done[b->ctrl_i]);
+	if (e == cudaSuccess) return 1;
+	if (e == cudaErrorNotReady) return 0;
+	g_last_error = std::string("ab_batch_ready: ") + cudaGetErrorString(e);
+	return AB_E_CUDA;
 }
 
 ab_transform * ab_batch_slot(ab_batch * b, int slot)

@@ -16,16 +16,26 @@
 //                    test rolls back to its last verified state.
 // Squarings of all admitted tests run together, one graph launch per chunk
 // and size class; the host steps between phases use the slot's transform.
+//
+// Admission is a pipeline: set-up threads classify each submitted test and
+// do the host half of its slot's set-up (gcd(N, R), N^-1 mod R: about 0.5 s
+// of GMP at 20 M bits) while the GPU squares the admitted ones; advance()
+// installs finished set-ups into free slots.  Each size class keeps up to two
+// chunks in flight on its own stream and is relaunched as soon as it can be,
+// so small classes are not held to the pace of large ones.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -85,8 +95,20 @@ struct Job
 	std::vector<uint8_t> vsnap, stash;
 	bool injected = false;
 
+	// admission, written by a set-up thread and read by the runner once the
+	// job is handed back: decided without a transform (early, with its
+	// message), the host half of the slot's set-up and N's size class, or
+	// the error that set-up met
+	bool early = false;
+	std::string early_msg;
+	ab_prepared * prep = nullptr;
+	ab_params p{};
+	int gcd_failed = 0;
+	int prep_rc = AB_OK;
+	std::string prep_err;
+
 	Job() { mpz_inits(N, E, res, chk, nullptr); }
-	~Job() { mpz_clears(N, E, res, chk, nullptr); }
+	~Job() { ab_prepared_destroy(prep); mpz_clears(N, E, res, chk, nullptr); }
 
 	// bit that the next squaring of the current phase uses, and its multiplier
 	uint32_t mult_at(long bit) const
@@ -125,22 +147,43 @@ std::string hex64(uint64_t u)
 struct ab_runner
 {
 	ab_runner_options o{};
-	std::deque<Job *> queue;
+	std::deque<Job *> queue;           // submitted, not yet handed to set-up
 	std::deque<Job *> done;
 	std::vector<std::unique_ptr<Class>> classes;
 	size_t used = 0;
 	uint64_t squarings = 0;
 	uint64_t tick = 0;                 // advance() calls
 
+	// set-up threads and their queues
+	std::vector<std::thread> workers;
+	std::mutex mu;
+	std::condition_variable cv_work, cv_ready;
+	std::deque<Job *> todo, ready;     // guarded by mu
+	int working = 0;                   // guarded by mu
+	bool stopping = false;             // guarded by mu
+	std::deque<Job *> prepared;        // set up, waiting for a slot
+	size_t outstanding = 0;            // handed to set-up, not yet in a slot or decided
+	size_t prepared_bytes = 0;         // host memory held by `prepared`
+
+	// set-up runs at most this far ahead of the free slots
+	static constexpr size_t max_ahead = 1024;
+	static constexpr size_t max_ahead_bytes = size_t(1) << 30;
+
 	~ab_runner()
 	{
+		{
+			std::lock_guard<std::mutex> lk(mu);
+			stopping = true;
+		}
+		cv_work.notify_all();
+		for (auto & t : workers) t.join();
 		for (auto & c : classes)
 		{
 			for (Job * j : c->slots) delete j;
 			ab_batch_destroy(c->b);
 		}
-		for (Job * j : queue) delete j;
-		for (Job * j : done) delete j;
+		for (auto * q : {&queue, &done, &todo, &ready, &prepared})
+			for (Job * j : *q) delete j;
 	}
 
 	void finish(Job * j, int status, const char * msg)
@@ -151,20 +194,21 @@ struct ab_runner
 		done.push_back(j);
 	}
 
-	// host part of admission: trivial cases, base, parameters; returns false
-	// when the job was decided without a transform
-	bool classify(Job * j, ab_params & p)
+	// set-up thread: trivial cases, the Euler base, then the host half of the
+	// slot's set-up (no CUDA call here)
+	static void prepare_job(Job * j)
 	{
 		const mpz_srcptr n = j->N;
 		if (mpz_sizeinbase(n, 2) <= 50 && mpz_cmp_ui(n, 999999999999999ul) <= 0)
 		{
-			j->r.decided_early = 1;
 			const int pp = mpz_probab_prime_p(n, 20);
+			j->r.decided_early = 1;
 			j->r.is_prp = pp != 0;
-			finish(j, 0, (pp != 0) ? "N is a probable prime." : "N is composite.");
-			return false;
+			j->early = true;
+			j->early_msg = (pp != 0) ? "N is a probable prime." : "N is composite.";
+			return;
 		}
-		if (mpz_even_p(n)) { j->r.decided_early = 1; finish(j, 0, "N is even."); return false; }
+		if (mpz_even_p(n)) { j->r.decided_early = 1; j->early = true; j->early_msg = "N is even."; return; }
 		if (j->euler)
 		{
 			int32_t a = 2;
@@ -177,8 +221,74 @@ struct ab_runner
 			j->a = a;
 		}
 		j->r.base = j->a;
-		ck(ab_probe(j->limbs.data(), j->limbs.size(), j->a, nullptr, &p, nullptr));
-		return true;
+		j->prep_rc = ab_batch_prepare(j->limbs.data(), j->limbs.size(), j->a, &j->prep, &j->p, &j->gcd_failed);
+		if (j->prep_rc != AB_OK) j->prep_err = ab_last_error();
+	}
+
+	void worker()
+	{
+		std::unique_lock<std::mutex> lk(mu);
+		for (;;)
+		{
+			cv_work.wait(lk, [&] { return stopping || !todo.empty(); });
+			if (stopping) return;
+			Job * j = todo.front(); todo.pop_front();
+			++working;
+			lk.unlock();
+			prepare_job(j);
+			lk.lock();
+			--working;
+			ready.push_back(j);
+			cv_ready.notify_all();
+		}
+	}
+
+	// hands queued tests to the set-up threads, as far ahead as the bounds allow
+	void feed()
+	{
+		std::vector<Job *> batch;
+		while (!queue.empty() && outstanding < max_ahead && prepared_bytes < max_ahead_bytes)
+		{
+			batch.push_back(queue.front());
+			queue.pop_front();
+			++outstanding;
+		}
+		if (batch.empty()) return;
+		if (workers.empty())
+		{
+			const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+			const unsigned nt = std::min(16u, std::max(1u, hw / 2));
+			for (unsigned t = 0; t < nt; ++t) workers.emplace_back([this] { worker(); });
+		}
+		{
+			std::lock_guard<std::mutex> lk(mu);
+			for (Job * j : batch) todo.push_back(j);
+		}
+		cv_work.notify_all();
+	}
+
+	// takes the finished set-ups; with wait_all, first waits until the set-up
+	// threads have none left (the GPU has nothing to run meanwhile)
+	void collect(bool wait_all)
+	{
+		std::deque<Job *> got;
+		{
+			std::unique_lock<std::mutex> lk(mu);
+			if (wait_all) cv_ready.wait(lk, [&] { return todo.empty() && working == 0; });
+			got.swap(ready);
+		}
+		for (Job * j : got)
+		{
+			prepared.push_back(j);
+			prepared_bytes += ab_prepared_bytes(j->prep);
+		}
+	}
+
+	size_t live_slots() const
+	{
+		size_t a = 0;
+		for (auto & c : classes) for (Job * j : c->slots) a += (j != nullptr);
+		return a;
 	}
 
 	// frees batches that hold no test, least recently used first, until `need`
@@ -228,86 +338,66 @@ struct ab_runner
 		return classes.back().get();
 	}
 
-	// Admission: classify queued tests, reserve a slot of their size class
-	// (creating the class within the HBM budget), then load each class's new
-	// slots together (host set-up on threads) and start their tests.
-	void admit()
+	// Admission: the set-up tests go into free slots of their size class (a
+	// class is created within the HBM budget), in submission order; the
+	// others wait for a slot
+	void install()
 	{
 		std::deque<Job *> later;
-		struct Pending { Class * c; int slot; Job * j; };
-		std::vector<Pending> pend;
-		while (!queue.empty())
+		while (!prepared.empty())
 		{
-			Job * j = queue.front(); queue.pop_front();
-			ab_params p{};
-			if (j->ph == MAIN && j->B == 0)
+			Job * j = prepared.front(); prepared.pop_front();
+			if (j->early || j->prep_rc != AB_OK || j->gcd_failed)
 			{
-				if (!classify(j, p)) continue;
-				j->r.K = p.K; j->r.pck = p.pck; j->r.ln = p.ln; j->r.lbase = p.lbase;
-				j->B = -1;     // classified
+				prepared_bytes -= ab_prepared_bytes(j->prep);
+				--outstanding;
+				if (j->early) { finish(j, 0, j->early_msg.c_str()); continue; }
+				if (j->prep_rc != AB_OK)
+				{
+					const std::string m = "the test could not be set up: " + j->prep_err;
+					finish(j, -1, m.c_str());
+					continue;
+				}
+				std::vector<uint64_t> f(j->limbs.size() + 2);
+				size_t fc = 0;
+				ck(ab_prepared_factor(j->prep, f.data(), f.size(), &fc));
+				mpz_t z; mpz_init(z); mpz_import(z, fc, -1, 8, 0, 0, f.data());
+				char * str = mpz_get_str(nullptr, 10, z);
+				char msg[256]; std::snprintf(msg, sizeof(msg), "%.200s divides N.", str);
+				free(str); mpz_clear(z);
+				j->r.decided_early = 1;
+				finish(j, 0, msg);
+				continue;
 			}
-			else { p.K = j->r.K; p.pck = j->r.pck; p.ln = j->r.ln; p.lbase = j->r.lbase; }
+			const ab_params & p = j->p;
+			j->r.K = p.K; j->r.pck = p.pck; j->r.ln = p.ln; j->r.lbase = p.lbase;
 			Class * c = class_for(p, true);
 			if (c == nullptr) { later.push_back(j); continue; }
 			const int slot = (int)(std::find(c->slots.begin(), c->slots.end(), nullptr) - c->slots.begin());
-			c->slots[slot] = j;                   // reserved
-			pend.push_back({c, slot, j});
-		}
-		queue.swap(later);
-
-		std::vector<Class *> order;
-		for (const Pending & q : pend) if (std::find(order.begin(), order.end(), q.c) == order.end()) order.push_back(q.c);
-		for (Class * c : order)
-		{
-			std::vector<Pending> mine;
-			for (const Pending & q : pend) if (q.c == c) mine.push_back(q);
-			const int cnt = (int)mine.size();
-			std::vector<int> slots(cnt), failed(cnt, 0);
-			std::vector<const uint64_t *> nl(cnt);
-			std::vector<size_t> nn(cnt);
-			std::vector<int32_t> aa(cnt);
-			for (int i = 0; i < cnt; ++i)
+			prepared_bytes -= ab_prepared_bytes(j->prep);
+			--outstanding;
+			ab_prepared * pp = j->prep;
+			j->prep = nullptr;
+			ck(ab_batch_install(c->b, slot, pp));
+			c->slots[slot] = j;
+			ab_transform * v = ab_batch_slot(c->b, slot);
+			ck(ab_set1(v));
+			ck(ab_copy(v, 1, 0));
+			if (!c->tuned)
 			{
-				slots[i] = mine[i].slot; nl[i] = mine[i].j->limbs.data(); nn[i] = mine[i].j->limbs.size(); aa[i] = mine[i].j->a;
+				int lb = 0;
+				if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
+				c->tuned = true;
 			}
-			ck(ab_batch_load_many(c->b, cnt, slots.data(), nl.data(), nn.data(), aa.data(), failed.data()));
-			for (int i = 0; i < cnt; ++i)
-			{
-				Job * j = mine[i].j;
-				const int slot = mine[i].slot;
-				ab_transform * v = ab_batch_slot(c->b, slot);
-				if (failed[i])
-				{
-					std::vector<uint64_t> f(j->limbs.size() + 2);
-					size_t fc = 0;
-					ck(ab_get_factor(v, f.data(), f.size(), &fc));
-					ab_batch_release(c->b, slot);
-					c->slots[slot] = nullptr;
-					mpz_t z; mpz_init(z); mpz_import(z, fc, -1, 8, 0, 0, f.data());
-					char * s = mpz_get_str(nullptr, 10, z);
-					char msg[256]; std::snprintf(msg, sizeof(msg), "%.200s divides N.", s);
-					free(s); mpz_clear(z);
-					j->r.decided_early = 1;
-					finish(j, 0, msg);
-					continue;
-				}
-				ck(ab_set1(v));
-				ck(ab_copy(v, 1, 0));
-				if (!c->tuned)
-				{
-					int lb = 0;
-					if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
-					c->tuned = true;
-				}
-				mpz_sub_ui(j->E, j->N, 1);
-				if (j->euler) mpz_fdiv_q_2exp(j->E, j->E, 1);
-				j->B = gl_block_size(mpz_sizeinbase(j->E, 2));
-				j->r.gl_block = j->B;
-				j->i = (long)mpz_sizeinbase(j->E, 2) - 1;
-				j->ph = MAIN;
-				if (o.gl_check_blocks > 0) { j->vsnap = payload(v); j->vi = j->i + 1; }
-			}
+			mpz_sub_ui(j->E, j->N, 1);
+			if (j->euler) mpz_fdiv_q_2exp(j->E, j->E, 1);
+			j->B = gl_block_size(mpz_sizeinbase(j->E, 2));
+			j->r.gl_block = j->B;
+			j->i = (long)mpz_sizeinbase(j->E, 2) - 1;
+			j->ph = MAIN;
+			if (o.gl_check_blocks > 0) { j->vsnap = payload(v); j->vi = j->i + 1; }
 		}
+		prepared.swap(later);
 	}
 
 	static std::vector<uint8_t> payload(ab_transform * v)
@@ -561,20 +651,38 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 	try
 	{
 		++r->tick;
-		r->admit();
-		std::vector<Class *> ran;
-		for (auto & c : r->classes) if (r->launch_class(*c)) ran.push_back(c.get());
-		for (Class * c : ran) r->settle_class(*c);
+		r->feed();
+		// with nothing on the GPU, wait for the set-ups in progress
+		r->collect(r->live_slots() == 0 && r->outstanding > r->prepared.size());
+		r->install();
+		r->feed();
+		// one chunk for every class that can take one without waiting; when
+		// none can, poll for up to 2 ms
+		const auto t0 = std::chrono::steady_clock::now();
+		for (;;)
+		{
+			bool launched = false, busy = false;
+			for (auto & c : r->classes)
+			{
+				if (std::all_of(c->slots.begin(), c->slots.end(), [](Job * j) { return j == nullptr; })) continue;
+				busy = true;
+				const int rd = ab_batch_ready(c->b);
+				if (rd < 0) throw rt_error(ab_last_error());
+				if (rd == 0) continue;
+				if (r->launch_class(*c)) { r->settle_class(*c); launched = true; }
+			}
+			if (launched || !busy) break;
+			if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(2)) break;
+			std::this_thread::sleep_for(std::chrono::microseconds(20));
+		}
 	}
 	catch (const std::exception & e)
 	{
 		std::fprintf(stderr, "ab_runner_advance: %s\n", e.what());
 		return AB_E_CUDA;
 	}
-	int a = 0;
-	for (auto & c : r->classes) for (Job * j : c->slots) a += (j != nullptr);
-	if (active) *active = a;
-	if (queued) *queued = (int)r->queue.size();
+	if (active) *active = (int)r->live_slots();
+	if (queued) *queued = (int)(r->queue.size() + r->outstanding);
 	return AB_OK;
 }
 

@@ -39,6 +39,19 @@ int ab_batch_load(ab_batch * b, int slot, const uint64_t * N, size_t nlimbs, int
    receives one flag per candidate. */
 int ab_batch_load_many(ab_batch * b, int count, const int * slots, const uint64_t * const * N, const size_t * nlimbs,
                        const int32_t * a, int * init_failed);
+/* ab_batch_load in two halves, for schedulers that overlap set-up with
+   squarings.  ab_batch_prepare is the host half (parameters, gcd(N, R),
+   N^-1 mod R, register words: a GMP computation of about 0.5 s at 20 M bits);
+   it makes no CUDA call and may run on any thread.  params (nullable)
+   receives N's size class; init_failed (nullable) is 1 when gcd(N, R) != 1,
+   and ab_prepared_factor then gives that gcd.  ab_batch_install is the device
+   half; it takes ownership of p, also when it fails. */
+typedef struct ab_prepared ab_prepared;
+int ab_batch_prepare(const uint64_t * N, size_t nlimbs, int32_t a, ab_prepared ** out, ab_params * params, int * init_failed);
+int ab_prepared_factor(const ab_prepared * p, uint64_t * out, size_t cap, size_t * count);
+size_t ab_prepared_bytes(const ab_prepared * p);     /* host memory it holds */
+void ab_prepared_destroy(ab_prepared * p);
+int ab_batch_install(ab_batch * b, int slot, ab_prepared * p);
 ab_transform * ab_batch_slot(ab_batch * b, int slot);
 /* Slot dst becomes a copy of loaded slot src (same N and base, registers
    included) without the host set-up: for re-tests and throughput runs. */
@@ -49,6 +62,9 @@ int ab_batch_release(ab_batch * b, int slot);
    squaring, keep Reg0 for the Gerbicz-Li product; ab_batch_gl_mul(slot) then
    does Reg1 *= kept value. */
 int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t * snap);
+/* 1 when ab_batch_steps would queue its chunk without waiting (at most two
+   chunks of a batch are in flight), 0 when it would wait, < 0 on error. */
+int ab_batch_ready(const ab_batch * b);
 int ab_batch_gl_mul(ab_batch * b, int slot);
 /* Row levels per row pass (0 = default split); used by the autotuner. */
 int ab_batch_set_geometry(ab_batch * b, int lb);
@@ -84,8 +100,15 @@ int ab_runner_create(const ab_runner_options * o, ab_runner ** out);
 void ab_runner_destroy(ab_runner * r);
 /* Queues a PRP test (Fermat base `base`, 0 = 2; or Euler). */
 int ab_runner_submit(ab_runner * r, const uint64_t * N, size_t nlimbs, int euler, int32_t base, uint64_t tag);
-/* Admits queued tests into free slots, then runs one chunk of every batch and
-   the host steps of the tests that reached the end of a phase. */
+/* Admits tests whose set-up is done into free slots, then queues one chunk of
+   squarings for every batch that can take one without waiting (each batch
+   keeps up to two in flight) and the host steps of the tests that reached the
+   end of a phase.  Set-up (the Euler base, gcd(N, R), N^-1 mod R) runs on host
+   threads of the runner, ahead of the free slots; when no test is on the GPU,
+   the call waits for the set-ups in progress.  Returns within about 2 ms
+   otherwise.  active: tests in slots; queued: tests submitted and not yet in a
+   slot.  A test whose set-up fails (e.g. N too large) finishes with status -1
+   and the error in its message. */
 int ab_runner_advance(ab_runner * r, int * active, int * queued);
 /* Waits for the work queued by ab_runner_advance on every batch. */
 int ab_runner_synchronize(ab_runner * r);

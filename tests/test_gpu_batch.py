@@ -240,3 +240,35 @@ def test_runner_frees_idle_batches_for_other_sizes():
     for tag, N in ((1, small), (2, big)):
         solo = A.prp_check(N, base=3)
         assert res[tag]["status"] == 0 and res[tag]["res64"] == solo["res64"]
+
+
+def test_prepare_then_install_equals_load():
+    # the two halves of ab_batch_load, the host half on another thread
+    import ctypes as C
+    import threading
+    cls = (5, 4, 12)
+    (N, _), = _same_class_numbers(cls, 1, 200000, 280000, 12)
+    L = A.lib()
+    limbs = A.int_to_limbs(N)
+    out = {}
+
+    def host_half():
+        p, prm, failed = C.c_void_p(), A.Params(), C.c_int()
+        out["rc"] = L.ab_batch_prepare(limbs.ctypes.data_as(A._u64p), len(limbs), 3, C.byref(p), C.byref(prm), C.byref(failed))
+        out["p"], out["cls"], out["failed"] = p, (prm.K, prm.pck, prm.ln), failed.value
+    th = threading.Thread(target=host_half)
+    th.start()
+    th.join()
+    assert out["rc"] == A.AB_OK and out["cls"] == cls and out["failed"] == 0
+    b = A.Batch(cls + (0,), capacity=2, max_steps=8)
+    assert L.ab_batch_ready(b.h) == 1
+    A._check(L.ab_batch_install(b.h, 1, out["p"]))           # takes ownership
+    b.load(0, N, 3)
+    for s in (0, 1):
+        b.slot(s).set1()
+    mult = np.full((8, 2), 3, dtype=np.uint32)
+    b.steps(mult)
+    assert np.array_equal(b.slot(0).read_register(0), b.slot(1).read_register(0))
+    assert b.slot(1).get(0) == pow(3, 255, N)
+    b.synchronize()
+    assert L.ab_batch_ready(b.h) == 1
