@@ -263,6 +263,7 @@ def test_prepare_then_install_equals_load():
     b = A.Batch(cls + (0,), capacity=2, max_steps=8)
     assert L.ab_batch_ready(b.h) == 1
     A._check(L.ab_batch_install(b.h, 1, out["p"]))           # takes ownership
+    b.Ns[1], b.bases[1] = N, 3                                # what the Python wrapper keeps for get()
     b.load(0, N, 3)
     for s in (0, 1):
         b.slot(s).set1()
