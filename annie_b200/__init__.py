@@ -80,6 +80,10 @@ class RunnerOptions(C.Structure):
                 ("inject_word", C.c_uint32)]
 
 
+class RunnerClass(C.Structure):
+    _fields_ = [("cls", Params), ("slots", C.c_int), ("active", C.c_int), ("squarings", C.c_uint64), ("chunks", C.c_uint64)]
+
+
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
 _u8p = C.POINTER(C.c_uint8)
@@ -152,6 +156,8 @@ ABI = [
     ("ab_runner_synchronize", [C.c_void_p], C.c_int),
     ("ab_runner_poll", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(PrpResult)], C.c_int),
     ("ab_runner_stats", [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_int)], C.c_int),
+    ("ab_runner_classes", [C.c_void_p, C.POINTER(RunnerClass), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    ("ab_runner_host_seconds", [C.c_void_p, C.POINTER(C.c_double)], C.c_int),
     ("ab_diag_forward", [C.c_void_p, C.c_int, _u32p, _u32p], C.c_int),
     ("ab_diag_product", [C.c_void_p, C.c_int, _u32p, _u32p, C.c_uint32, _u32p, C.c_int, _u32p], C.c_int),
 ]
@@ -567,3 +573,18 @@ class Runner:
         s, l, b = C.c_uint64(), C.c_uint64(), C.c_int()
         _check(self.L.ab_runner_stats(self.h, C.byref(s), C.byref(l), C.byref(b)))
         return {"squarings": s.value, "launches": l.value, "batches": b.value}
+
+    def classes(self):
+        """Per size class: (K, pck, ln), slots, active tests, squarings, chunks."""
+        cnt = C.c_int()
+        _check(self.L.ab_runner_classes(self.h, None, 0, C.byref(cnt)))
+        arr = (RunnerClass * max(1, cnt.value))()
+        _check(self.L.ab_runner_classes(self.h, arr, cnt.value, C.byref(cnt)))
+        return [{"class": [x.cls.K, x.cls.pck, x.cls.ln], "slots": x.slots, "active": x.active,
+                 "squarings": x.squarings, "chunks": x.chunks} for x in arr[:cnt.value]]
+
+    def host_seconds(self):
+        """Host time inside advance(): admission, autotune, phase steps, sleeping."""
+        out = (C.c_double * 4)()
+        _check(self.L.ab_runner_host_seconds(self.h, out))
+        return dict(zip(("admission", "autotune", "phase_steps", "sleep"), [round(x, 3) for x in out]))

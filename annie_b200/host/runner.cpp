@@ -134,7 +134,11 @@ struct Class
 	bool tuned = false;
 	size_t bytes = 0;                  // device memory of the batch
 	uint64_t last_used = 0;            // runner tick of the last chunk or admission
+	uint64_t squarings = 0, chunks = 0;
 };
+
+using clk = std::chrono::steady_clock;
+double secs(clk::duration d) { return std::chrono::duration<double>(d).count(); }
 
 std::string hex64(uint64_t u)
 {
@@ -164,6 +168,7 @@ struct ab_runner
 	std::deque<Job *> prepared;        // set up, waiting for a slot
 	size_t outstanding = 0;            // handed to set-up, not yet in a slot or decided
 	size_t prepared_bytes = 0;         // host memory held by `prepared`
+	double host_s[4] = {};             // advance(): admission, autotune, host steps, waiting
 
 	// set-up runs at most this far ahead of the free slots
 	static constexpr size_t max_ahead = 1024;
@@ -386,7 +391,10 @@ struct ab_runner
 			if (!c->tuned)
 			{
 				int lb = 0;
-				if (o.autotune) ck(ab_batch_autotune(c->b, slot, o.chunk, &lb));
+				const auto t0 = clk::now();
+				// 16 squarings per split are enough to rank the splits
+				if (o.autotune) ck(ab_batch_autotune(c->b, slot, std::min(o.chunk, 16), &lb));
+				host_s[1] += secs(clk::now() - t0);
 				c->tuned = true;
 			}
 			mpz_sub_ui(j->E, j->N, 1);
@@ -560,6 +568,7 @@ struct ab_runner
 		if (!any) return false;
 		c.last_used = tick;
 		ck(ab_batch_steps(c.b, S, c.mult.data(), c.snap.data()));
+		++c.chunks;
 		return true;
 	}
 
@@ -588,6 +597,7 @@ struct ab_runner
 			j->i -= count[s];
 			j->r.squarings += count[s];
 			squarings += (uint64_t)count[s];
+			c.squarings += (uint64_t)count[s];
 			if (was_main && !j->injected && o.inject_bit >= 0 && j->tag == o.inject_tag && last <= o.inject_bit)
 			{
 				// host-side fault: one word of Reg0 changes between two launches
@@ -601,7 +611,12 @@ struct ab_runner
 				start_check(ab_batch_slot(c.b, s), j);
 				continue;
 			}
-			if (j->remaining() <= 0) next_phase(c, s, j);
+			if (j->remaining() <= 0)
+			{
+				const auto t0 = clk::now();
+				next_phase(c, s, j);
+				host_s[2] += secs(clk::now() - t0);
+			}
 		}
 	}
 };
@@ -653,9 +668,11 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 		++r->tick;
 		r->feed();
 		// with nothing on the GPU, wait for the set-ups in progress
+		const auto ta = clk::now();
 		r->collect(r->live_slots() == 0 && r->outstanding > r->prepared.size());
 		r->install();
 		r->feed();
+		r->host_s[0] += secs(clk::now() - ta);
 		// one chunk for every class that can take one without waiting; when
 		// none can, poll for up to 2 ms
 		const auto t0 = std::chrono::steady_clock::now();
@@ -673,7 +690,9 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 			}
 			if (launched || !busy) break;
 			if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(2)) break;
+			const auto tw = clk::now();
 			std::this_thread::sleep_for(std::chrono::microseconds(20));
+			r->host_s[3] += secs(clk::now() - tw);
 		}
 	}
 	catch (const std::exception & e)
@@ -705,6 +724,34 @@ int ab_runner_poll(ab_runner * r, uint64_t * tag, ab_prp_result * out)
 	if (out) *out = j->r;
 	delete j;
 	return 1;
+}
+
+int ab_runner_classes(const ab_runner * r, ab_runner_class * out, int cap, int * count)
+{
+	if (r == nullptr || count == nullptr || (cap > 0 && out == nullptr)) return AB_E_ARG;
+	int i = 0;
+	for (auto & c : r->classes)
+	{
+		if (i < cap)
+		{
+			ab_runner_class & x = out[i];
+			x.cls = c->cls;
+			x.slots = c->cap;
+			x.active = (int)std::count_if(c->slots.begin(), c->slots.end(), [](Job * j) { return j != nullptr; });
+			x.squarings = c->squarings;
+			x.chunks = c->chunks;
+		}
+		++i;
+	}
+	*count = i;
+	return AB_OK;
+}
+
+int ab_runner_host_seconds(const ab_runner * r, double * out)
+{
+	if (r == nullptr || out == nullptr) return AB_E_ARG;
+	for (int i = 0; i < 4; ++i) out[i] = r->host_s[i];
+	return AB_OK;
 }
 
 int ab_runner_stats(const ab_runner * r, uint64_t * squarings, uint64_t * launches, int * batches)

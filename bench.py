@@ -523,6 +523,7 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0):
     # end finish here, and their time counts
     served_s = time.perf_counter() - t0
     sq_served = r.stats()["squarings"]
+    classes, host_s = r.classes(), r.host_seconds()
     r.close()
     # plain: first come first served, one test at a time; a timer stops the
     # running test at the window's end (ab_prp_quit: it returns as aborted)
@@ -558,7 +559,8 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0):
         same &= (res["res64"], res["is_prp"], res["status"]) == (alone["res64"], alone["is_prp"], alone["status"])
     return {"rate_per_s": rate, "requests": len(reqs), "window_s": window,
             "served": {"squarings_per_s": round(sq_served / served_s, 1), "completed": len(served),
-                       "censored": len(reqs) - len(served), "p50_s": _pct(lat_s, 0.5), "p99_s": _pct(lat_s, 0.99)},
+                       "censored": len(reqs) - len(served), "p50_s": _pct(lat_s, 0.5), "p99_s": _pct(lat_s, 0.99),
+                       "host_s": host_s, "classes": classes},
             "plain": {"squarings_per_s": round(sq_plain / window, 1), "completed": len(plain),
                       "censored": len(reqs) - len(plain), "p50_s": _pct(lat_p, 0.5), "p99_s": _pct(lat_p, 0.99)},
             "throughput_vs_plain": round((sq_served / served_s) / max(1e-9, sq_plain / window), 3),

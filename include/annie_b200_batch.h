@@ -117,6 +117,23 @@ int ab_runner_poll(ab_runner * r, uint64_t * tag, ab_prp_result * out);
 /* Squarings executed for tests since creation (all slots). */
 int ab_runner_stats(const ab_runner * r, uint64_t * squarings, uint64_t * launches, int * batches);
 
+/* Per size class (batch) of the runner, for monitoring. */
+typedef struct
+{
+	ab_params cls;             /* K, pck, ln (lbase 0) */
+	int slots;                 /* capacity of the class's batch */
+	int active;                /* tests in its slots */
+	uint64_t squarings;        /* squarings run for its tests */
+	uint64_t chunks;           /* chunks (graph launches) queued */
+} ab_runner_class;
+/* Fills up to cap entries; count receives the number of classes. */
+int ab_runner_classes(const ab_runner * r, ab_runner_class * out, int cap, int * count);
+/* Host seconds spent inside ab_runner_advance since creation: out[0]
+   admission (installing set-ups, autotuning included), out[1] autotuning,
+   out[2] host steps between phases, out[3] sleeping while no batch could
+   take a chunk. */
+int ab_runner_host_seconds(const ab_runner * r, double * out);
+
 #ifdef __cplusplus
 }
 #endif
