@@ -489,7 +489,7 @@ def _pct(v, q):
     return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
 
 
-def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0):
+def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True, slots=64):
     """One Poisson stream served for a fixed window two ways, on the same GPU:
     the continuous-batching runner, and the one-at-a-time path (each test run
     to completion in arrival order, the last one stopped at the window's end).
@@ -500,7 +500,7 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0):
     reqs = _serve_stream(rate, window, lo, hi, seed)
     # served: requests are submitted as they arrive, the runner advances
     # continuously until the window ends
-    r = A.Runner(chunk=32, max_slots_per_class=64, gl_check_blocks=gl_check_blocks)
+    r = A.Runner(chunk=32, max_slots_per_class=slots, gl_check_blocks=gl_check_blocks, autotune=autotune)
     t0 = time.perf_counter()
     served, nxt, lat_s = {}, 0, []
     while True:
@@ -573,7 +573,8 @@ def run_serve_workload(args):
     second and p50/p99 time-to-result of the continuous-batching runner against
     the one-at-a-time path on the same stream."""
     lo, hi = args.serve_bits
-    out_rates = [serve_one_rate(rate, args.serve_window, lo, hi, int(rate * 1000) + 7) for rate in args.serve_rates]
+    out_rates = [serve_one_rate(rate, args.serve_window, lo, hi, int(rate * 1000) + 7, autotune=not args.serve_no_autotune,
+                                slots=args.serve_slots) for rate in args.serve_rates]
     head = max(out_rates, key=lambda x: x["throughput_vs_plain"])
     return {"metric": "served_squarings_per_s", "value": head["served"]["squarings_per_s"], "unit": "squarings/s", "n_gpus": 1,
             "steps": len(out_rates), "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -814,6 +815,8 @@ def main():
     ap.add_argument("--serve-bits", type=int, nargs=2, default=[100000, 20000000])
     ap.add_argument("--serve-window", type=float, default=60.0)
     ap.add_argument("--side-serve-window", type=float, default=40.0)
+    ap.add_argument("--serve-no-autotune", action="store_true", help="serve: size classes keep the default split")
+    ap.add_argument("--serve-slots", type=int, default=64, help="serve: slots per size class")
     ap.add_argument("--side-serve-rate", type=float, default=1.0)
     ap.add_argument("--proth-squarings", type=int, default=100000)
     ap.add_argument("--proth-n", type=int, default=2000000)
