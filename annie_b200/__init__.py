@@ -77,7 +77,7 @@ BENCH_TABLE_E = [33216, 83048, 166092, 332190, 664381, 1162672, 1660962, 3321924
 class RunnerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots_per_class", C.c_int), ("chunk", C.c_int),
                 ("autotune", C.c_int), ("gl_check_blocks", C.c_int), ("inject_tag", C.c_uint64), ("inject_bit", C.c_int64),
-                ("inject_word", C.c_uint32)]
+                ("inject_word", C.c_uint32), ("latency_ln", C.c_int), ("epoch_us", C.c_int)]
 
 
 class RunnerClass(C.Structure):
@@ -526,7 +526,7 @@ class Runner:
     """Continuous-batching PRP runner: submit tests, advance, poll results."""
 
     def __init__(self, device=0, hbm_budget_bytes=32 << 30, max_slots_per_class=256, chunk=64, autotune=True,
-                 gl_check_blocks=0, inject_tag=0, inject_bit=-1, inject_word=0):
+                 gl_check_blocks=0, inject_tag=0, inject_bit=-1, inject_word=0, latency_ln=0, epoch_us=20000):
         self.L = lib()
         o = RunnerOptions()
         self.L.ab_runner_options_default(C.byref(o))
@@ -534,6 +534,7 @@ class Runner:
         o.autotune = int(bool(autotune))
         o.gl_check_blocks = gl_check_blocks
         o.inject_tag, o.inject_bit, o.inject_word = inject_tag, inject_bit, inject_word
+        o.latency_ln, o.epoch_us = latency_ln, epoch_us
         h = C.c_void_p()
         _check(self.L.ab_runner_create(C.byref(o), C.byref(h)))
         self.h = h

@@ -818,6 +818,7 @@ struct ab_batch
 	u32 * h_ctrl[2] = {};              // page-locked staging, alternating between launches
 	cudaEvent_t ctrl_done[2] = {};     // the upload out of h_ctrl[i] has completed
 	int ctrl_i = 0;
+	cudaEvent_t chunk_done = nullptr;  // the last chunk has completed
 	std::vector<ab_transform *> views;
 	cudaGraphExec_t gexec = nullptr;
 	int g_steps = 0;
@@ -833,6 +834,7 @@ struct ab_batch
 		if (d_cand) cudaFree(d_cand);
 		if (d_ctrl) cudaFree(d_ctrl);
 		for (int i = 0; i < 2; ++i) { if (h_ctrl[i]) cudaFreeHost(h_ctrl[i]); if (ctrl_done[i]) cudaEventDestroy(ctrl_done[i]); }
+		if (chunk_done) cudaEventDestroy(chunk_done);
 		if (st) cudaStreamDestroy(st);
 	}
 
@@ -1383,6 +1385,8 @@ int ab_batch_create(int device, const ab_params * cls, int capacity, int max_ste
 			CK(cudaEventCreateWithFlags(&b->ctrl_done[i], cudaEventDisableTiming));
 			CK(cudaEventRecord(b->ctrl_done[i], b->st));
 		}
+		CK(cudaEventCreateWithFlags(&b->chunk_done, cudaEventDisableTiming));
+		CK(cudaEventRecord(b->chunk_done, b->st));
 		b->views.assign(capacity, nullptr);
 		// constants of the class (the digit size comes from d_cand)
 		ab_params p = *cls; p.lbase = 17;
@@ -1558,11 +1562,17 @@ int ab_batch_install(ab_batch * b, int slot, ab_prepared * p)
 int ab_batch_ready(const ab_batch * b)
 {
 	if (b == nullptr) return AB_E_ARG;
-	const cudaError_t e = cudaEventQuery(b->ctrl_done[b->ctrl_i]);
-	if (e == cudaSuccess) return 1;
-	if (e == cudaErrorNotReady) return 0;
-	g_last_error = std::string("ab_batch_ready: ") + cudaGetErrorString(e);
-	return AB_E_CUDA;
+	for (int i = 0; i < 2; ++i)
+	{
+		const cudaError_t e = cudaEventQuery(i == 0 ? b->chunk_done : b->ctrl_done[b->ctrl_i]);
+		if (e == cudaSuccess) return 2 - i;
+		if (e != cudaErrorNotReady)
+		{
+			g_last_error = std::string("ab_batch_ready: ") + cudaGetErrorString(e);
+			return AB_E_CUDA;
+		}
+	}
+	return 0;
 }
 
 ab_transform * ab_batch_slot(ab_batch * b, int slot)
@@ -1659,6 +1669,7 @@ int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t
 			b->g_kernels = b->recorded;
 		}
 		CK(cudaGraphLaunch(b->gexec, b->st));
+		CK(cudaEventRecord(b->chunk_done, b->st));
 		b->launches += b->g_kernels;                  // kernels of the graph
 		for (ab_transform * v : b->views) if (v) v->prefwd = false;
 	});

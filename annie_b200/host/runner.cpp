@@ -170,6 +170,32 @@ struct ab_runner
 	size_t prepared_bytes = 0;         // host memory held by `prepared`
 	double host_s[4] = {};             // advance(): admission, autotune, host steps, waiting
 
+	// latency epochs (latency_ln > 0): whose turn it is, since when
+	bool small_turn = true;
+	clk::time_point epoch_t0{};
+
+	bool is_small(const Class & c) const { return c.cls.ln <= o.latency_ln; }
+
+	static bool has_tests(const Class & c)
+	{
+		return std::any_of(c.slots.begin(), c.slots.end(), [](Job * j) { return j != nullptr; });
+	}
+
+	// the turn passes to the other group when its epoch is over or it has no
+	// tests left
+	void pick_turn()
+	{
+		bool has[2] = {false, false};
+		for (auto & c : classes) if (has_tests(*c)) has[is_small(*c) ? 1 : 0] = true;
+		const auto now = clk::now();
+		const bool other = has[small_turn ? 0 : 1], mine = has[small_turn ? 1 : 0];
+		if (other && (!mine || now - epoch_t0 > std::chrono::microseconds(o.epoch_us)))
+		{
+			small_turn = !small_turn;
+			epoch_t0 = now;
+		}
+	}
+
 	// set-up runs at most this far ahead of the free slots
 	static constexpr size_t max_ahead = 1024;
 	static constexpr size_t max_ahead_bytes = size_t(1) << 30;
@@ -632,6 +658,8 @@ void ab_runner_options_default(ab_runner_options * o)
 	o->autotune = 1;
 	o->gl_check_blocks = 0;
 	o->inject_bit = -1;
+	o->latency_ln = 0;
+	o->epoch_us = 20000;
 }
 
 int ab_runner_create(const ab_runner_options * o, ab_runner ** out)
@@ -639,7 +667,11 @@ int ab_runner_create(const ab_runner_options * o, ab_runner ** out)
 	if (out == nullptr) return AB_E_ARG;
 	ab_runner * r = new ab_runner();
 	if (o) r->o = *o; else ab_runner_options_default(&r->o);
-	if (r->o.chunk < 1 || r->o.max_slots_per_class < 1) { delete r; return AB_E_ARG; }
+	if (r->o.chunk < 1 || r->o.max_slots_per_class < 1 || r->o.latency_ln < 0 || (r->o.latency_ln > 0 && r->o.epoch_us < 1))
+	{
+		delete r;
+		return AB_E_ARG;
+	}
 	*out = r;
 	return AB_OK;
 }
@@ -675,17 +707,22 @@ int ab_runner_advance(ab_runner * r, int * active, int * queued)
 		r->host_s[0] += secs(clk::now() - ta);
 		// one chunk for every class that can take one without waiting; when
 		// none can, poll for up to 2 ms
+		// (with latency epochs, only the classes whose turn it is, the large
+		// ones when their last chunk is done)
+		const bool epochs = r->o.latency_ln > 0;
 		const auto t0 = std::chrono::steady_clock::now();
 		for (;;)
 		{
 			bool launched = false, busy = false;
+			if (epochs) r->pick_turn();
 			for (auto & c : r->classes)
 			{
-				if (std::all_of(c->slots.begin(), c->slots.end(), [](Job * j) { return j == nullptr; })) continue;
+				if (!ab_runner::has_tests(*c)) continue;
 				busy = true;
+				if (epochs && r->is_small(*c) != r->small_turn) continue;
 				const int rd = ab_batch_ready(c->b);
 				if (rd < 0) throw rt_error(ab_last_error());
-				if (rd == 0) continue;
+				if (rd == 0 || (epochs && !r->is_small(*c) && rd < 2)) continue;
 				if (r->launch_class(*c)) { r->settle_class(*c); launched = true; }
 			}
 			if (launched || !busy) break;

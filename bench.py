@@ -489,7 +489,7 @@ def _pct(v, q):
     return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
 
 
-def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True, slots=64):
+def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True, slots=64, latency_ln=0, epoch_us=20000):
     """One Poisson stream served for a fixed window two ways, on the same GPU:
     the continuous-batching runner, and the one-at-a-time path (each test run
     to completion in arrival order, the last one stopped at the window's end).
@@ -500,7 +500,8 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True,
     reqs = _serve_stream(rate, window, lo, hi, seed)
     # served: requests are submitted as they arrive, the runner advances
     # continuously until the window ends
-    r = A.Runner(chunk=32, max_slots_per_class=slots, gl_check_blocks=gl_check_blocks, autotune=autotune)
+    r = A.Runner(chunk=32, max_slots_per_class=slots, gl_check_blocks=gl_check_blocks, autotune=autotune,
+                 latency_ln=latency_ln, epoch_us=epoch_us)
     t0 = time.perf_counter()
     served, nxt, lat_s = {}, 0, []
     while True:
@@ -532,7 +533,7 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True,
     stop = threading.Timer(window, L.ab_prp_quit)
     t0 = time.perf_counter()
     stop.start()
-    plain, lat_p, sq_plain = {}, [], 0
+    plain, lat_p, sq_plain, words_plain = {}, [], 0, 0
     for i, (ta, N, euler, base) in enumerate(reqs):
         now = time.perf_counter() - t0
         if now >= window:
@@ -543,6 +544,7 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True,
                 break
         res = A.prp_check(N, euler=euler, base=base)
         sq_plain += res["squarings"]
+        words_plain += res["squarings"] * (res["K"] + 1) << res["ln"]
         if res["status"] == 2:                     # stopped at the window's end
             break
         plain[i] = res
@@ -557,13 +559,19 @@ def serve_one_rate(rate, window, lo, hi, seed, gl_check_blocks=0, autotune=True,
             _, N, euler, base = reqs[tag]
             alone = A.prp_check(N, euler=euler, base=base)
         same &= (res["res64"], res["is_prp"], res["status"]) == (alone["res64"], alone["is_prp"], alone["status"])
+    # work-normalised throughput: transform words squared per second (a
+    # squaring of class (K, ln) transforms (K + 1) 2^ln words)
+    words_served = sum(c["squarings"] * (c["class"][0] + 1) << c["class"][2] for c in classes)
     return {"rate_per_s": rate, "requests": len(reqs), "window_s": window,
+            "policy": {"latency_ln": latency_ln, "epoch_us": epoch_us if latency_ln else None, "autotune": autotune,
+                       "slots_per_class": slots},
             "served": {"squarings_per_s": round(sq_served / served_s, 1), "completed": len(served),
                        "censored": len(reqs) - len(served), "p50_s": _pct(lat_s, 0.5), "p99_s": _pct(lat_s, 0.99),
                        "host_s": host_s, "classes": classes},
             "plain": {"squarings_per_s": round(sq_plain / window, 1), "completed": len(plain),
                       "censored": len(reqs) - len(plain), "p50_s": _pct(lat_p, 0.5), "p99_s": _pct(lat_p, 0.99)},
             "throughput_vs_plain": round((sq_served / served_s) / max(1e-9, sq_plain / window), 3),
+            "gwords_per_s": {"served": round(words_served / served_s / 1e9, 3), "plain": round(words_plain / window / 1e9, 3)},
             "results_equal_alone": bool(same)}
 
 
@@ -574,7 +582,8 @@ def run_serve_workload(args):
     the one-at-a-time path on the same stream."""
     lo, hi = args.serve_bits
     out_rates = [serve_one_rate(rate, args.serve_window, lo, hi, int(rate * 1000) + 7, autotune=not args.serve_no_autotune,
-                                slots=args.serve_slots) for rate in args.serve_rates]
+                                slots=args.serve_slots, latency_ln=args.serve_latency_ln, epoch_us=args.serve_epoch_us)
+                 for rate in args.serve_rates]
     head = max(out_rates, key=lambda x: x["throughput_vs_plain"])
     return {"metric": "served_squarings_per_s", "value": head["served"]["squarings_per_s"], "unit": "squarings/s", "n_gpus": 1,
             "steps": len(out_rates), "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -817,6 +826,9 @@ def main():
     ap.add_argument("--side-serve-window", type=float, default=40.0)
     ap.add_argument("--serve-no-autotune", action="store_true", help="serve: size classes keep the default split")
     ap.add_argument("--serve-slots", type=int, default=64, help="serve: slots per size class")
+    ap.add_argument("--serve-latency-ln", type=int, default=0,
+                    help="serve: classes with ln <= this take turns with the larger ones (0 = all together)")
+    ap.add_argument("--serve-epoch-us", type=int, default=20000)
     ap.add_argument("--side-serve-rate", type=float, default=1.0)
     ap.add_argument("--proth-squarings", type=int, default=100000)
     ap.add_argument("--proth-n", type=int, default=2000000)

@@ -62,8 +62,9 @@ int ab_batch_release(ab_batch * b, int slot);
    squaring, keep Reg0 for the Gerbicz-Li product; ab_batch_gl_mul(slot) then
    does Reg1 *= kept value. */
 int ab_batch_steps(ab_batch * b, int steps, const uint32_t * mult, const uint8_t * snap);
-/* 1 when ab_batch_steps would queue its chunk without waiting (at most two
-   chunks of a batch are in flight), 0 when it would wait, < 0 on error. */
+/* 2 when the batch's last chunk has completed, 1 when ab_batch_steps would
+   queue its chunk without waiting (at most two chunks of a batch are in
+   flight), 0 when it would wait, < 0 on error. */
 int ab_batch_ready(const ab_batch * b);
 int ab_batch_gl_mul(ab_batch * b, int slot);
 /* Row levels per row pass (0 = default split); used by the autotuner. */
@@ -93,6 +94,12 @@ typedef struct
 	                              Reg0 changed (ab_inject_word) once its loop passes bit inject_bit */
 	int64_t inject_bit;        /* -1 = no injection */
 	uint32_t inject_word;
+	int latency_ln;            /* > 0: size classes with ln <= latency_ln (short squarings, latency-bound
+	                              launches) and the larger ones take turns on the GPU in epochs of
+	                              epoch_us microseconds, the larger ones with one chunk in flight, so
+	                              that the short launches do not queue behind large grids; 0 = all
+	                              classes run together */
+	int epoch_us;
 } ab_runner_options;
 
 void ab_runner_options_default(ab_runner_options * o);
