@@ -826,7 +826,7 @@ def main():
     ap.add_argument("--side-serve-window", type=float, default=40.0)
     ap.add_argument("--serve-no-autotune", action="store_true", help="serve: size classes keep the default split")
     ap.add_argument("--serve-slots", type=int, default=64, help="serve: slots per size class")
-    ap.add_argument("--serve-latency-ln", type=int, default=0,
+    ap.add_argument("--serve-latency-ln", type=int, default=14,
                     help="serve: classes with ln <= this take turns with the larger ones (0 = all together)")
     ap.add_argument("--serve-epoch-us", type=int, default=20000)
     ap.add_argument("--side-serve-rate", type=float, default=1.0)
@@ -891,7 +891,8 @@ def main():
         line["proth2M"] = side_proth2m(args)
         line["batch"] = side_batch(args)
         lo, hi = args.serve_bits
-        line["serve"] = serve_one_rate(args.side_serve_rate, args.side_serve_window, lo, hi, 1007)
+        line["serve"] = serve_one_rate(args.side_serve_rate, args.side_serve_window, lo, hi, 1007,
+                                       latency_ln=args.serve_latency_ln, epoch_us=args.serve_epoch_us)
     print(json.dumps(line), flush=True)
     if line["parity"]["checked"] and not line["parity"]["equal"]:
         sys.stderr.write("PARITY FAILURE: registers differ from the reference after the window\n")
