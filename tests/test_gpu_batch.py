@@ -80,14 +80,19 @@ def _run_all(runner, limit=200000):
     return results
 
 
-def test_runner_matches_reference_golden_and_solo():
+@pytest.mark.parametrize("latency_ln", [0, 10])
+def test_runner_matches_reference_golden_and_solo(latency_ln):
+    # latency_ln 10: the smaller classes and the larger ones take turns (1 ms epochs)
     with open(os.path.join(HERE, "golden", "prp_vectors.json")) as f:
         vec = [v for v in json.load(f) if not v.get("big")]
     jobs = {}
     for tag, v in enumerate(vec):
         N = random_N(v["bits"], v["seed"]) if v["form"] == "random_odd" else proth_N(v["n"], v["seed"])[1]
         jobs[tag] = (N, v)
-    r = A.Runner(chunk=32, max_slots_per_class=8)
+    r = A.Runner(chunk=32, max_slots_per_class=8, latency_ln=latency_ln, epoch_us=1000)
+    if latency_ln:
+        lns = {A.probe(N, v["base"] or 2)[0][2] for N, v in jobs.values()}
+        assert min(lns) <= latency_ln < max(lns)                 # both groups present
     for tag, (N, v) in jobs.items():
         r.submit(N, euler=bool(v["euler"]), base=v["base"], tag=tag)
     res = _run_all(r)
