@@ -148,6 +148,12 @@ ABI = [
     ("ab_batch_autotune", [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)], C.c_int),
     ("ab_batch_synchronize", [C.c_void_p], C.c_int),
     ("ab_batch_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
+    ("ab_mixed_create", [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    ("ab_mixed_destroy", [C.c_void_p], None),
+    ("ab_mixed_steps", [C.c_void_p, C.c_int, C.POINTER(_u32p), C.POINTER(_u8p)], C.c_int),
+    ("ab_mixed_ready", [C.c_void_p], C.c_int),
+    ("ab_mixed_synchronize", [C.c_void_p], C.c_int),
+    ("ab_mixed_launch_count", [C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
     ("ab_runner_options_default", [C.POINTER(RunnerOptions)], None),
     ("ab_runner_create", [C.POINTER(RunnerOptions), C.POINTER(C.c_void_p)], C.c_int),
     ("ab_runner_destroy", [C.c_void_p], None),
@@ -519,6 +525,55 @@ class Batch:
     def launch_count(self):
         c = C.c_uint64()
         _check(self.L.ab_batch_launch_count(self.h, C.byref(c)))
+        return c.value
+
+
+class Mixed:
+    """A mixed-size group of batches (include/annie_b200_batch.h, ab_mixed_*):
+    their squarings run together, one launch per pass for every class."""
+
+    def __init__(self, batches, max_steps=64):
+        self.L = lib()
+        self.batches = list(batches)
+        arr = (C.c_void_p * len(self.batches))(*[b.h.value for b in self.batches])
+        h = C.c_void_p()
+        _check(self.L.ab_mixed_create(arr, len(self.batches), max_steps, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ab_mixed_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def steps(self, mults, snaps=None):
+        """mults[i]: (steps, capacity_i) multipliers of batch i; snaps[i] the same
+        shape of 0/1 flags (nullable)."""
+        ms = [np.ascontiguousarray(m, dtype=np.uint32) for m in mults]
+        steps = ms[0].shape[0]
+        assert all(m.shape == (steps, b.capacity) for m, b in zip(ms, self.batches))
+        mp = (_u32p * len(ms))(*[m.ctypes.data_as(_u32p) for m in ms])
+        sp = None
+        if snaps is not None:
+            ss = [None if x is None else np.ascontiguousarray(x, dtype=np.uint8) for x in snaps]
+            sp = (_u8p * len(ss))(*[_u8p() if x is None else x.ctypes.data_as(_u8p) for x in ss])
+            self._keep = ss
+        _check(self.L.ab_mixed_steps(self.h, steps, mp, sp))
+
+    def ready(self):
+        return self.L.ab_mixed_ready(self.h)
+
+    def synchronize(self):
+        _check(self.L.ab_mixed_synchronize(self.h))
+
+    def launch_count(self):
+        c = C.c_uint64()
+        _check(self.L.ab_mixed_launch_count(self.h, C.byref(c)))
         return c.value
 
 

@@ -848,10 +848,15 @@ struct ab_batch
 	}
 
 	uint64_t recorded = 0;              // kernels recorded by rows()/cols() (graph nodes)
+	int geo_version = 0;               // changes with the split (a mixed group then re-records)
+	// when set, rows() and cols() append their passes here instead of launching
+	struct Pass { bool row; RowJobs rj; ColJobs cj; int nj; };
+	std::vector<Pass> * sink = nullptr;
 	void rows(const RowJob & j0, const RowJob * j1 = nullptr)
 	{
 		RowJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
 		const int nj = j1 ? 2 : 1;
+		if (sink) { Pass q{}; q.row = true; q.rj = js; q.nj = nj; sink->push_back(q); return; }
 		if (geo.G > 0) { CK(launch_midpass(geo, tc, js, nj, st, zl, false)); ++recorded; }
 		CK(launch_rowpass(geo, tc, js, nj, st, zl));
 		++recorded;
@@ -860,6 +865,7 @@ struct ab_batch
 	void cols(const ColJob & j0, const ColJob * j1 = nullptr)
 	{
 		ColJobs js; js.j[0] = j0; js.j[1] = j1 ? *j1 : j0;
+		if (sink) { Pass q{}; q.row = false; q.cj = js; q.nj = j1 ? 2 : 1; sink->push_back(q); return; }
 		CK(launch_colpass(geo, tc, js, j1 ? 2 : 1, st, zl));
 		++recorded;
 	}
@@ -1683,6 +1689,7 @@ int ab_batch_set_geometry(ab_batch * b, int lb)
 		if (!make_geometry(b->cls.ln, lb, g)) throw ab_error(AB_E_ARG, "geometry not available for this length");
 		CK(cudaStreamSynchronize(b->st));
 		b->geo = g;
+		++b->geo_version;
 		apply_geometry(b->tc, g);
 		for (ab_transform * v : b->views) if (v) { v->use_geometry(g); v->prefwd = false; }
 		RowJobs rjs{}; ColJobs cjs{};
@@ -1770,6 +1777,287 @@ int ab_batch_synchronize(ab_batch * b)
 int ab_batch_launch_count(const ab_batch * b, uint64_t * count)
 {
 	return guarded([&] { if (b == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); *count = b->launches; });
+}
+
+}
+
+// ============================================================ mixed-size groups
+// Batches of different size classes squared together: each pass of a chunk
+// (the initial forward column levels, then per squaring the six row and
+// column passes of the batch schedule) is one launch over the candidates of
+// every class, driven by a device table of per-class jobs (FusedRowPass /
+// FusedColPass).  The passes are the ones each batch would launch itself,
+// recorded through its sink, so a slot's results do not depend on the group.
+struct ab_mixed
+{
+	int device = 0;
+	cudaStream_t st = nullptr;
+	std::vector<ab_batch *> b;
+	int max_steps = 0;
+	TConst * d_tc = nullptr;
+	FusedRowPass * d_row = nullptr;
+	FusedColPass * d_col = nullptr;
+	std::vector<u32 *> h_ctrl[2];      // per batch: page-locked control staging, alternating
+	cudaEvent_t ctrl_done[2] = {};
+	int ctrl_i = 0;
+	cudaEvent_t chunk_done = nullptr, ev_join = nullptr;
+	cudaGraphExec_t gexec = nullptr;
+	int g_steps = 0;
+	std::vector<int> g_zl, g_ver;
+	uint64_t g_kernels = 0, launches = 0;
+
+	~ab_mixed()
+	{
+		if (gexec) cudaGraphExecDestroy(gexec);
+		if (d_tc) cudaFree(d_tc);
+		if (d_row) cudaFree(d_row);
+		if (d_col) cudaFree(d_col);
+		for (int i = 0; i < 2; ++i)
+		{
+			for (u32 * h : h_ctrl[i]) if (h) cudaFreeHost(h);
+			if (ctrl_done[i]) cudaEventDestroy(ctrl_done[i]);
+		}
+		if (chunk_done) cudaEventDestroy(chunk_done);
+		if (ev_join) cudaEventDestroy(ev_join);
+		if (st) cudaStreamDestroy(st);
+	}
+
+	// records the passes of `steps` squarings of every batch and captures them
+	// as fused launches
+	void capture(int steps, const std::vector<int> & zl)
+	{
+		const int nc = (int)b.size();
+		std::vector<std::vector<ab_batch::Pass>> lists(nc);
+		for (int i = 0; i < nc; ++i)
+		{
+			b[i]->sink = &lists[i];
+			try { b[i]->record_steps(steps); }
+			catch (...) { b[i]->sink = nullptr; throw; }
+			b[i]->sink = nullptr;
+		}
+		const size_t np = lists[0].size();
+		for (int i = 1; i < nc; ++i)
+		{
+			if (lists[i].size() != np) throw ab_error(AB_E_ARG, "batches of a group record different schedules");
+			for (size_t q = 0; q < np; ++q)
+				if (lists[i][q].row != lists[0][q].row) throw ab_error(AB_E_ARG, "batches of a group record different schedules");
+		}
+		std::vector<FusedRowPass> hr;
+		std::vector<FusedColPass> hc;
+		std::vector<u32> ctas;
+		size_t smem_row = 0, smem_col = 0;
+		for (int i = 0; i < nc; ++i)
+		{
+			smem_row = std::max(smem_row, fused_rowpass_smem(b[i]->geo.LB + 1));
+			smem_col = std::max(smem_col, colpass_smem(b[i]->geo, b[i]->cls.K + 1));
+		}
+		for (size_t q = 0; q < np; ++q)
+		{
+			if (lists[0][q].row)
+			{
+				FusedRowPass f; std::memset(&f, 0, sizeof(f));
+				f.nclass = nc;
+				for (int i = 0; i < nc; ++i)
+				{
+					const ab_batch & x = *b[i];
+					f.nbx[i] = (u32)(x.cls.K + 1) * x.geo.HR;
+					f.njobs[i] = (u32)lists[i][q].nj;
+					f.log_r[i] = x.geo.LB + 1;
+					f.jobs[i] = lists[i][q].rj;
+					f.begin[i + 1] = f.begin[i] + f.nbx[i] * f.njobs[i] * (u32)zl[i];
+				}
+				ctas.push_back(f.begin[nc]);
+				hr.push_back(f);
+			}
+			else
+			{
+				FusedColPass f; std::memset(&f, 0, sizeof(f));
+				f.nclass = nc;
+				for (int i = 0; i < nc; ++i)
+				{
+					const ab_batch & x = *b[i];
+					f.nbx[i] = x.geo.RC / (u32)x.geo.C;
+					f.njobs[i] = (u32)lists[i][q].nj;
+					f.sel[i] = x.geo.LA * 8 + x.cls.K;
+					f.jobs[i] = lists[i][q].cj;
+					f.begin[i + 1] = f.begin[i] + f.nbx[i] * f.njobs[i] * (u32)zl[i];
+				}
+				ctas.push_back(f.begin[nc]);
+				hc.push_back(f);
+			}
+		}
+		if (hr.size() > (size_t)3 * max_steps || hc.size() > (size_t)3 * max_steps + 1) throw ab_error(AB_E_ARG, "schedule longer than the group's tables");
+		std::vector<TConst> tcs(nc);
+		for (int i = 0; i < nc; ++i) tcs[i] = b[i]->tc;
+		CK(cudaMemcpyAsync(d_tc, tcs.data(), sizeof(TConst) * nc, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(d_row, hr.data(), sizeof(FusedRowPass) * hr.size(), cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(d_col, hc.data(), sizeof(FusedColPass) * hc.size(), cudaMemcpyHostToDevice, st));
+		CK(cudaStreamSynchronize(st));
+		// kernel attributes before the capture
+		CK(launch_fused_rowpass(d_row, d_tc, 0, smem_row, st));
+		CK(launch_fused_colpass(d_col, d_tc, 0, smem_col, st));
+		if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+		cudaGraph_t g = nullptr;
+		g_kernels = 0;
+		CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		try
+		{
+			size_t ri = 0, ci = 0;
+			for (size_t q = 0; q < np; ++q)
+			{
+				if (ctas[q] == 0) { (lists[0][q].row ? ri : ci)++; continue; }
+				if (lists[0][q].row) CK(launch_fused_rowpass(d_row + ri++, d_tc, ctas[q], smem_row, st));
+				else CK(launch_fused_colpass(d_col + ci++, d_tc, ctas[q], smem_col, st));
+				++g_kernels;
+			}
+		}
+		catch (...) { cudaStreamEndCapture(st, &g); if (g) cudaGraphDestroy(g); throw; }
+		CK(cudaStreamEndCapture(st, &g));
+		const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+		cudaGraphDestroy(g);
+		CK(e);
+		g_steps = steps;
+		g_zl = zl;
+		g_ver.clear();
+		for (ab_batch * x : b) g_ver.push_back(x->geo_version);
+	}
+};
+
+extern "C" {
+
+int ab_mixed_create(ab_batch * const * batches, int count, int max_steps, ab_mixed ** out)
+{
+	if (out) *out = nullptr;
+	ab_mixed * m = nullptr;
+	const int rc = guarded([&] {
+		if (batches == nullptr || out == nullptr || count < 1 || count > AB_FUSE_MAXC || max_steps < 1) throw ab_error(AB_E_ARG, "bad arguments");
+		for (int i = 0; i < count; ++i)
+		{
+			const ab_batch * x = batches[i];
+			if (x == nullptr || x->device != batches[0]->device || max_steps > x->max_steps) throw ab_error(AB_E_ARG, "bad arguments");
+			if (x->geo.G > 0) throw ab_error(AB_E_UNSUPPORTED, "a group takes lengths up to 2^20");
+			for (int j = 0; j < i; ++j) if (batches[j] == x) throw ab_error(AB_E_ARG, "a batch is named twice");
+		}
+		m = new ab_mixed();
+		m->device = batches[0]->device;
+		m->b.assign(batches, batches + count);
+		m->max_steps = max_steps;
+		CK(cudaSetDevice(m->device));
+		int least = 0, greatest = 0;
+		CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+		CK(cudaStreamCreateWithPriority(&m->st, cudaStreamNonBlocking, greatest));
+		CK(cudaMalloc(&m->d_tc, sizeof(TConst) * count));
+		CK(cudaMalloc(&m->d_row, sizeof(FusedRowPass) * 3 * max_steps));
+		CK(cudaMalloc(&m->d_col, sizeof(FusedColPass) * (3 * max_steps + 1)));
+		for (int i = 0; i < 2; ++i)
+		{
+			for (ab_batch * x : m->b)
+			{
+				u32 * h = nullptr;
+				CK(cudaMallocHost(&h, (size_t)3 * max_steps * x->cap * 4));
+				m->h_ctrl[i].push_back(h);
+			}
+			CK(cudaEventCreateWithFlags(&m->ctrl_done[i], cudaEventDisableTiming));
+			CK(cudaEventRecord(m->ctrl_done[i], m->st));
+		}
+		CK(cudaEventCreateWithFlags(&m->chunk_done, cudaEventDisableTiming));
+		CK(cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming));
+		CK(cudaEventRecord(m->chunk_done, m->st));
+	});
+	if (rc != AB_OK) { delete m; return rc; }
+	*out = m;
+	return AB_OK;
+}
+
+void ab_mixed_destroy(ab_mixed * m)
+{
+	if (m) cudaStreamSynchronize(m->st);
+	delete m;
+}
+
+int ab_mixed_steps(ab_mixed * m, int steps, const uint32_t * const * mult, const uint8_t * const * snap)
+{
+	return guarded([&] {
+		if (m == nullptr || mult == nullptr || steps < 1 || steps > m->max_steps) throw ab_error(AB_E_ARG, "bad arguments");
+		const int nc = (int)m->b.size();
+		std::vector<int> zl(nc, 0);
+		bool any = false;
+		for (int i = 0; i < nc; ++i)
+		{
+			const ab_batch & x = *m->b[i];
+			if (mult[i] == nullptr) throw ab_error(AB_E_ARG, "bad arguments");
+			int top = 0;
+			for (int c = 0; c < x.cap; ++c)
+				if (x.views[c] != nullptr && !x.views[c]->failed)
+					for (int s = 0; s < steps; ++s) if (mult[i][(size_t)s * x.cap + c] != 0u) { top = c + 1; break; }
+			int z = (top > 0) ? 1 : 0;
+			while (z < top) z <<= 1;
+			zl[i] = std::min(z, x.cap);
+			any |= top > 0;
+		}
+		if (!any) return;
+		// control words: the staging used two chunks ago must have been uploaded
+		const int hi = m->ctrl_i;
+		CK(cudaEventSynchronize(m->ctrl_done[hi]));
+		for (int i = 0; i < nc; ++i)
+		{
+			ab_batch & x = *m->b[i];
+			u32 * const hc = m->h_ctrl[hi][i];
+			const int cap = x.cap;
+			for (int s = 0; s < steps; ++s)
+				for (int c = 0; c < cap; ++c)
+				{
+					const bool live = x.views[c] != nullptr && !x.views[c]->failed;
+					const u32 mv = live ? mult[i][(size_t)s * cap + c] : 0u;
+					hc[((size_t)s * 3 + 0) * cap + c] = mv;
+					hc[((size_t)s * 3 + 1) * cap + c] = (mv != 0u) ? 1u : 0u;
+					hc[((size_t)s * 3 + 2) * cap + c] = (snap != nullptr && snap[i] != nullptr && mv != 0u && snap[i][(size_t)s * cap + c]) ? 1u : 0u;
+				}
+			// the batch's own work (loads, Gerbicz-Li products, reads) comes first
+			CK(cudaEventRecord(m->ev_join, x.st));
+			CK(cudaStreamWaitEvent(m->st, m->ev_join, 0));
+			CK(cudaMemcpyAsync(x.d_ctrl, hc, (size_t)3 * steps * cap * 4, cudaMemcpyHostToDevice, m->st));
+		}
+		CK(cudaEventRecord(m->ctrl_done[hi], m->st));
+		m->ctrl_i ^= 1;
+		bool same = (m->gexec != nullptr && m->g_steps == steps && m->g_zl == zl);
+		for (int i = 0; same && i < nc; ++i) same = (m->g_ver[i] == m->b[i]->geo_version);
+		if (!same) m->capture(steps, zl);
+		CK(cudaGraphLaunch(m->gexec, m->st));
+		CK(cudaEventRecord(m->chunk_done, m->st));
+		m->launches += m->g_kernels;
+		for (ab_batch * x : m->b)
+		{
+			CK(cudaStreamWaitEvent(x->st, m->chunk_done, 0));
+			for (ab_transform * v : x->views) if (v) v->prefwd = false;
+		}
+	});
+}
+
+int ab_mixed_ready(const ab_mixed * m)
+{
+	if (m == nullptr) return AB_E_ARG;
+	for (int i = 0; i < 2; ++i)
+	{
+		const cudaError_t e = cudaEventQuery(i == 0 ? m->chunk_done : m->ctrl_done[m->ctrl_i]);
+		if (e == cudaSuccess) return 2 - i;
+		if (e != cudaErrorNotReady)
+		{
+			g_last_error = std::string("ab_mixed_ready: ") + cudaGetErrorString(e);
+			return AB_E_CUDA;
+		}
+	}
+	return 0;
+}
+
+int ab_mixed_synchronize(ab_mixed * m)
+{
+	return guarded([&] { if (m == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); CK(cudaStreamSynchronize(m->st)); });
+}
+
+int ab_mixed_launch_count(const ab_mixed * m, uint64_t * count)
+{
+	return guarded([&] { if (m == nullptr || count == nullptr) throw ab_error(AB_E_ARG, "bad arguments"); *count = m->launches; });
 }
 
 }

@@ -254,22 +254,23 @@ struct RowCfg
 	static constexpr size_t SMEM = sizeof(u32) * ((1u << LOG_R) + (1u << LOG_R) / 16);   // padded row
 };
 
-template <int LOG_R>
-__global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowpass(const RowJobs jobs, const TConst c)
+// The row pass of row bx (prime k = bx / HR, row r) of candidate cand, by P
+// threads (tid < P) sharing the padded row buffer sm.  When P exceeds the
+// row's virtual threads T, the threads above T only take part in the
+// barriers.  mask_nt: threads of the CTA, for the shuffle masks.
+template <int LOG_R, u32 P>
+__device__ __forceinline__ void rowpass_body(const RowJob & J, const TConst & c, u32 cand, u32 bx, u32 tid, u32 * sm, u32 mask_nt)
 {
 	constexpr int LB = LOG_R - 1;
-	constexpr u32 T = RowCfg<LOG_R>::T, NT = RowCfg<LOG_R>::NT, RND = RowCfg<LOG_R>::RND;
+	constexpr u32 T = RowCfg<LOG_R>::T, NT = P, RND = (T + P - 1) / P;
+	constexpr bool IDLE = P > T;                                  // some threads have no virtual thread
 	constexpr int NL = LB - 4;                                    // levels above the last stage
 	constexpr int S0 = (NL % 4 == 0) ? 4 : NL % 4;                // first stage (when NL > 0)
 	constexpr int NS = (NL == 0) ? 0 : 1 + (NL - S0) / 4;        // stages above the last
 	constexpr int B0 = LB + 1 - S0;
-	extern __shared__ __align__(16) u32 sm[];
 
-	const RowJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
-	const u32 cand = blockIdx.z;
-	if (J.active != nullptr && J.active[cand] == 0u) return;
 	const size_t cofs = (size_t)cand * J.stride;
-	const u32 k = blockIdx.x / c.HR, r = blockIdx.x - k * c.HR;
+	const u32 k = bx / c.HR, r = bx - k * c.HR;
 	const u32 p = c.p[k], p2 = 2 * p, pinv = c.pinv[k];
 	u32 * __restrict__ x = J.x + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R);
 	RowTw tw;
@@ -278,7 +279,8 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 	tw.H = c.HR;
 	const u32 * __restrict__ xp = (J.mode == ROW_MUL) ? J.xp + cofs + (size_t)k * c.n + (size_t)r * (1u << LOG_R) : nullptr;
 	const u32 Hr = c.HR + r;
-	const u32 tid = threadIdx.x;
+	// threads of a shuffle: with idle threads, only the first T of the first warp
+	const u32 mnt = (IDLE && T < 32) ? T : mask_nt;
 	u32 v[RP_EPT];
 	// twiddles of the last forward level of virtual thread vt: the c of its polynomials
 	auto w1 = [&](u32 vt) { return tw.w + (Hr << (LB - 1)) + ((vt >> 1) << 3); };
@@ -291,11 +293,12 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 		for (u32 rr = 0; rr < RND; ++rr)
 		{
 			const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 			rp_load_global<4>(v, x, vt, T, 1);
 			rp_radix<4, false>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			if (J.mode != ROW_FWD_ONLY)
 			{
-				rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1(vt), p, p2, pinv);
+				rp_pointwise(v, xp, J.mode == ROW_MUL, vt, mnt, w1(vt), p, p2, pinv);
 				rp_radix<4, true>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			}
 			else reduce_all(v, p2);
@@ -310,6 +313,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 		for (u32 rr = 0; rr < RND; ++rr)
 		{
 			const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 			rp_load_global<S0>(v, x, vt, T, B0);
 			rp_radix<S0, false>(v, vt, T, B0, LB, tw, Hr, p, p2);
 			rp_store_smem<S0>(v, sm, vt, T, B0);
@@ -324,6 +328,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 			for (u32 rr = 0; rr < RND; ++rr)
 			{
 				const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 				rp_load_smem<4>(v, sm, vt, T, b);
 				rp_radix<4, false>(v, vt, T, b, LB, tw, Hr, p, p2);
 				rp_store_smem<4>(v, sm, vt, T, b);
@@ -336,6 +341,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 		for (u32 rr = 0; rr < RND; ++rr)
 		{
 			const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 			rp_load_smem<4>(v, sm, vt, T, 1);
 			rp_radix<4, false>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			if (J.mode == ROW_FWD_ONLY)
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 				rp_store_global<4>(v, x, vt, T, 1);
 				continue;
 			}
-			rp_pointwise(v, xp, J.mode == ROW_MUL, vt, NT, w1(vt), p, p2, pinv);
+			rp_pointwise(v, xp, J.mode == ROW_MUL, vt, mnt, w1(vt), p, p2, pinv);
 			rp_radix<4, true>(v, vt, T, 1, LB, tw, Hr, p, p2);
 			rp_store_smem<4>(v, sm, vt, T, 1);
 		}
@@ -361,6 +367,7 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 			for (u32 rr = 0; rr < RND; ++rr)
 			{
 				const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 				rp_load_smem<4>(v, sm, vt, T, b);
 				rp_radix<4, true>(v, vt, T, b, LB, tw, Hr, p, p2);
 				rp_store_smem<4>(v, sm, vt, T, b);
@@ -372,11 +379,22 @@ __global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowp
 		for (u32 rr = 0; rr < RND; ++rr)
 		{
 			const u32 vt = tid + rr * NT;
+			if (IDLE && vt >= T) continue;
 			rp_load_smem<S0>(v, sm, vt, T, B0);
 			rp_radix<S0, true>(v, vt, T, B0, LB, tw, Hr, p, p2);
 			rp_store_global<S0>(v, x, vt, T, B0);
 		}
 	}
+}
+
+template <int LOG_R>
+__global__ void __launch_bounds__(RowCfg<LOG_R>::NT, RowCfg<LOG_R>::MINB) k_rowpass(const RowJobs jobs, const TConst c)
+{
+	extern __shared__ __align__(16) u32 sm[];
+	const RowJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
+	const u32 cand = blockIdx.z;
+	if (J.active != nullptr && J.active[cand] == 0u) return;
+	rowpass_body<LOG_R, RowCfg<LOG_R>::NT>(J, c, cand, blockIdx.x, threadIdx.x, sm, RowCfg<LOG_R>::NT);
 }
 
 // ================================================================ column pass
@@ -544,20 +562,18 @@ __device__ __forceinline__ i32 carry_phase2(int lb, Big<L> f, const u32 (&d)[4][
 	return top;
 }
 
+// The column pass of column group b of nb (32 columns each) of candidate
+// cand, by all threads of the CTA; sm: colpass_smem bytes of shared memory.
 template <int LOG_H, int K, int PCK>
-__global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, const TConst c)
+__device__ __forceinline__ void colpass_body(ColJob J, const TConst & c, u32 cand, int b, int nb, u32 * sm, int & decision)
 {
 	constexpr int KP = K + 1, L = K;             // transform primes, limbs of the carry
 	constexpr int H = 1 << LOG_H;
 	constexpr int PS = H * TW;                   // tile plane stride
-	extern __shared__ __align__(16) u32 sm[];
 	u32 * const tile = sm;                       // [KP][H][TW]
 	u32 * const cw = tile + KP * PS;             // [H][TW/4][L] carry-out words
 	uint2 * const twc = reinterpret_cast<uint2 *>(cw + H * (TW / 4) * L);   // [3][KP][H] column twiddles
-	__shared__ int decision;
 
-	ColJob J = (blockIdx.y == 0) ? jobs.j[0] : jobs.j[1];
-	const u32 cand = blockIdx.z;
 	const u32 amul = (J.mult != nullptr) ? J.mult[cand] : J.a;
 	if (amul == 0u) return;                       // inactive batch slot
 	{
@@ -571,7 +587,6 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 	}
 	const int lb = (J.cand != nullptr) ? J.cand[cand].lbase : c.lbase;
 	const u32 R = c.R, n = c.n;
-	const int nb = (int)gridDim.x, b = (int)blockIdx.x;
 	const u32 c0 = (u32)b * CC;
 	const bool single = (nb == 1);
 	// predecessor columns: the 4 left of the CTA (the last 4 of the previous row
@@ -784,6 +799,95 @@ __global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, 
 		first = false;
 	}
 }
+
+template <int LOG_H, int K, int PCK>
+__global__ void __launch_bounds__(COL_THREADS, 2) k_colpass(const ColJobs jobs, const TConst c)
+{
+	extern __shared__ __align__(16) u32 sm[];
+	__shared__ int decision;
+	colpass_body<LOG_H, K, PCK>((blockIdx.y == 0) ? jobs.j[0] : jobs.j[1], c, blockIdx.z, (int)blockIdx.x, (int)gridDim.x, sm, decision);
+}
+
+// ================================================================ mixed-size passes
+// The class of CTA bid and the CTA's job, candidate and row / column group.
+struct FusedCta
+{
+	int ci;
+	u32 job, cand, bx;
+};
+
+template <typename Pass>
+__device__ __forceinline__ FusedCta fused_cta(const Pass * __restrict__ d, u32 bid)
+{
+	FusedCta f;
+	int ci = 0;
+	while (ci + 1 < d->nclass && bid >= d->begin[ci + 1]) ++ci;
+	const u32 local = bid - d->begin[ci], nbx = d->nbx[ci];
+	const u32 cj = local / nbx;
+	f.ci = ci;
+	f.bx = local - cj * nbx;
+	f.job = cj % d->njobs[ci];
+	f.cand = cj / d->njobs[ci];
+	return f;
+}
+
+// The class's constants into shared memory (they come from a table written
+// when the group was set up, so before griddep_wait).
+__device__ __forceinline__ void fused_consts(TConst & cs, const TConst * __restrict__ tcs, int ci)
+{
+	const u32 * src = reinterpret_cast<const u32 *>(tcs + ci);
+	u32 * dst = reinterpret_cast<u32 *>(&cs);
+	for (u32 i = threadIdx.x; i < sizeof(TConst) / 4; i += blockDim.x) dst[i] = __ldg(src + i);
+	__syncthreads();
+}
+
+__global__ void __launch_bounds__(AB_FUSED_ROW_THREADS, 4) k_fused_rowpass(const FusedRowPass * __restrict__ d, const TConst * __restrict__ tcs)
+{
+	extern __shared__ __align__(16) u32 sm[];
+	__shared__ TConst cs;
+	const FusedCta f = fused_cta(d, blockIdx.x);
+	const RowJob J = d->jobs[f.ci].j[f.job];
+	if (J.active != nullptr && J.active[f.cand] == 0u) return;
+	fused_consts(cs, tcs, f.ci);
+	constexpr u32 P = AB_FUSED_ROW_THREADS;
+	switch (d->log_r[f.ci])
+	{
+	case 5: rowpass_body<5, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 6: rowpass_body<6, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 7: rowpass_body<7, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 8: rowpass_body<8, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 9: rowpass_body<9, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 10: rowpass_body<10, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 11: rowpass_body<11, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 12: rowpass_body<12, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 13: rowpass_body<13, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	case 14: rowpass_body<14, P>(J, cs, f.cand, f.bx, threadIdx.x, sm, P); break;
+	default: break;
+	}
+}
+
+#define AB_FUSED_COL(LH, KK, PP) \
+	case LH * 8 + KK: colpass_body<LH, KK, PP>(J, cs, f.cand, (int)f.bx, (int)d->nbx[f.ci], sm, decision); break;
+#define AB_FUSED_COL_K(LH) AB_FUSED_COL(LH, 2, 1) AB_FUSED_COL(LH, 3, 2) AB_FUSED_COL(LH, 4, 2) AB_FUSED_COL(LH, 5, 4)
+
+__global__ void __launch_bounds__(COL_THREADS, 2) k_fused_colpass(const FusedColPass * __restrict__ d, const TConst * __restrict__ tcs)
+{
+	extern __shared__ __align__(16) u32 sm[];
+	__shared__ TConst cs;
+	__shared__ int decision;
+	const FusedCta f = fused_cta(d, blockIdx.x);
+	const ColJob J = d->jobs[f.ci].j[f.job];
+	const u32 amul = (J.mult != nullptr) ? J.mult[f.cand] : J.a;
+	if (amul == 0u) return;                       // inactive batch slot
+	fused_consts(cs, tcs, f.ci);
+	switch (d->sel[f.ci])
+	{
+	AB_FUSED_COL_K(1) AB_FUSED_COL_K(2) AB_FUSED_COL_K(3) AB_FUSED_COL_K(4) AB_FUSED_COL_K(5) AB_FUSED_COL_K(6)
+	default: break;
+	}
+}
+#undef AB_FUSED_COL_K
+#undef AB_FUSED_COL
 
 // ================================================================ register words of the reference
 // Canonical residue of the exact value (d0, d1, d2) mod a reference prime:
@@ -1059,6 +1163,39 @@ cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs &
 	case 5: return colpass_k<5, 4>(g, c, jobs, njobs, s, ncand);
 	default: return cudaErrorInvalidValue;
 	}
+}
+
+size_t fused_rowpass_smem(int log_r)
+{
+	return sizeof(u32) * (((size_t)1 << log_r) + ((size_t)1 << log_r) / 16);
+}
+
+cudaError_t launch_fused_rowpass(const FusedRowPass * d, const TConst * tcs, u32 ctas, size_t smem, cudaStream_t s)
+{
+	static std::atomic<unsigned long long> attr_done{0};
+	static size_t set_smem = 0;
+	if (smem > set_smem)
+	{
+		attr_done.store(0);
+		set_smem = smem;
+	}
+	const cudaError_t e = allow_dynamic_smem(k_fused_rowpass, set_smem, attr_done);
+	if (e != cudaSuccess || ctas == 0) return e;
+	return launch_pdl(k_fused_rowpass, dim3(ctas), dim3(AB_FUSED_ROW_THREADS), smem, s, d, tcs);
+}
+
+cudaError_t launch_fused_colpass(const FusedColPass * d, const TConst * tcs, u32 ctas, size_t smem, cudaStream_t s)
+{
+	static std::atomic<unsigned long long> attr_done{0};
+	static size_t set_smem = 0;
+	if (smem > set_smem)
+	{
+		attr_done.store(0);
+		set_smem = smem;
+	}
+	const cudaError_t e = allow_dynamic_smem(k_fused_colpass, set_smem, attr_done);
+	if (e != cudaSuccess || ctas == 0) return e;
+	return launch_pdl(k_fused_colpass, dim3(ctas), dim3(COL_THREADS), smem, s, d, tcs);
 }
 
 cudaError_t launch_export(const RefConst & rc, const u32 * norm, u32 * words, u32 n, cudaStream_t s)

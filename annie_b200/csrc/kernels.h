@@ -99,6 +99,37 @@ cudaError_t launch_rowpass(const Geometry & g, const TConst & c, const RowJobs &
 cudaError_t launch_midpass(const Geometry & g, const TConst & c, const RowJobs & jobs, int njobs, cudaStream_t s, int ncand, bool inverse);
 cudaError_t launch_colpass(const Geometry & g, const TConst & c, const ColJobs & jobs, int njobs, cudaStream_t s, int ncand = 1);
 
+// Mixed-size passes: one launch runs the same pass for the candidates of
+// several size classes (lengths up to 2^20, no mid levels).  CTAs
+// [begin[i], begin[i+1]) belong to class i, nbx per job and candidate
+// (candidate-major, then job); each class has its own constants (tcs[i]),
+// jobs and row or column split.
+constexpr int AB_FUSE_MAXC = 16;
+constexpr unsigned AB_FUSED_ROW_THREADS = 256;
+struct FusedRowPass
+{
+	int nclass;
+	u32 begin[AB_FUSE_MAXC + 1];
+	u32 nbx[AB_FUSE_MAXC];        // KP HR rows
+	u32 njobs[AB_FUSE_MAXC];
+	int log_r[AB_FUSE_MAXC];      // row length 2^log_r (LB + 1)
+	RowJobs jobs[AB_FUSE_MAXC];
+};
+struct FusedColPass
+{
+	int nclass;
+	u32 begin[AB_FUSE_MAXC + 1];
+	u32 nbx[AB_FUSE_MAXC];        // RC / 32 column groups
+	u32 njobs[AB_FUSE_MAXC];
+	int sel[AB_FUSE_MAXC];        // LA * 8 + K
+	ColJobs jobs[AB_FUSE_MAXC];
+};
+// Shared memory of the fused row pass for rows of 2^log_r words.
+size_t fused_rowpass_smem(int log_r);
+// ctas: begin[nclass]; smem: the largest need of the classes.
+cudaError_t launch_fused_rowpass(const FusedRowPass * d, const TConst * tcs, u32 ctas, size_t smem, cudaStream_t s);
+cudaError_t launch_fused_colpass(const FusedColPass * d, const TConst * tcs, u32 ctas, size_t smem, cudaStream_t s);
+
 // Register words of the reference (K planes of residues mod its primes) from
 // the normal form, and back.  The import sets *bad when a coefficient's value
 // does not fit the 96-bit normal form (the words are not a normal-form

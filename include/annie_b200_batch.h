@@ -78,6 +78,23 @@ int ab_batch_autotune(ab_batch * b, int src, int steps, int * row_levels);
 int ab_batch_synchronize(ab_batch * b);
 int ab_batch_launch_count(const ab_batch * b, uint64_t * count);
 
+/* Mixed-size groups: batches of different size classes (NTT lengths up to
+   2^20) squared together.  Each pass of a chunk is one launch over the
+   candidates of every class of the group, which reads its per-class jobs
+   from a device table; the slots' results are those of ab_batch_steps on
+   each batch.  While in a group, a batch is stepped through the group only
+   (its slots stay usable with every ab_transform call, and
+   ab_batch_set_geometry makes the group re-record). */
+typedef struct ab_mixed ab_mixed;
+int ab_mixed_create(ab_batch * const * batches, int count, int max_steps, ab_mixed ** out);
+void ab_mixed_destroy(ab_mixed * m);
+/* mult[i], snap[i] (snap and snap[i] nullable): as ab_batch_steps for batch i. */
+int ab_mixed_steps(ab_mixed * m, int steps, const uint32_t * const * mult, const uint8_t * const * snap);
+/* As ab_batch_ready. */
+int ab_mixed_ready(const ab_mixed * m);
+int ab_mixed_synchronize(ab_mixed * m);
+int ab_mixed_launch_count(const ab_mixed * m, uint64_t * count);
+
 typedef struct ab_runner ab_runner;
 
 typedef struct

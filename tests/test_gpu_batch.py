@@ -278,3 +278,60 @@ def test_prepare_then_install_equals_load():
     assert b.slot(1).get(0) == pow(3, 255, N)
     b.synchronize()
     assert L.ab_batch_ready(b.h) == 1
+
+
+def test_mixed_group_equals_single_transforms():
+    # three size classes (three row lengths, K = 3, 4, 5) in one group: every
+    # pass is one launch over all of them; slots must equal single transforms
+    specs = [((5, 4, 12), 200000, 280000), ((4, 2, 11), 90000, 110000), ((3, 2, 9), 15000, 25000)]
+    batches, singles, caps = [], [], [3, 4, 2]
+    for ci, (cls, lo, hi) in enumerate(specs):
+        nums = _same_class_numbers(cls, 2, lo, hi, 30 + ci)
+        b = A.Batch(cls + (0,), capacity=caps[ci], max_steps=16)
+        row = []
+        for s, (N, _) in zip((0, caps[ci] - 1), nums):        # a gap between the loaded slots
+            assert not b.load(s, N, 3)
+            v = b.slot(s)
+            v.set1(); v.copy(1, 0)
+            t = A.Transform(N, 3)
+            t.set1(); t.copy(1, 0)
+            row.append((s, t))
+        batches.append(b)
+        singles.append(row)
+    m = A.Mixed(batches, max_steps=16)
+    rng = np.random.default_rng(11)
+    for rnd in range(3):
+        steps = 16 if rnd != 1 else 12                      # a second graph for a shorter chunk
+        mults, snaps = [], []
+        for ci, b in enumerate(batches):
+            mult = rng.choice([1, 3], size=(steps, caps[ci])).astype(np.uint32)
+            loaded = {s for s, _ in singles[ci]}
+            for s in range(caps[ci]):
+                if s not in loaded:
+                    mult[:, s] = 0
+            if ci == 1 and rnd == 2:
+                mult[steps - 4:, caps[ci] - 1] = 0             # sits the last steps out
+            snap = np.zeros((steps, caps[ci]), dtype=np.uint8)
+            snap[5, 0] = 1
+            mults.append(mult); snaps.append(snap)
+        m.steps(mults, snaps)
+        for ci, b in enumerate(batches):
+            b.gl_mul(0)
+            for s, t in singles[ci]:
+                for i in range(steps):
+                    if mults[ci][i, s]:
+                        t.square_mul(int(mults[ci][i, s]))
+                        if s == 0 and i == 5:
+                            t.copy(2, 0)
+                if s == 0:
+                    t.mul(1, 2)
+                v = b.slot(s)
+                assert np.array_equal(v.read_register(0), t.read_register(0)), "class %d slot %d Reg0, round %d" % (ci, s, rnd)
+                assert np.array_equal(v.read_register(1), t.read_register(1)), "class %d slot %d Reg1, round %d" % (ci, s, rnd)
+    assert m.launch_count() > 0
+    m.synchronize()
+    assert m.ready() == 2
+    for ci, b in enumerate(batches):
+        for s, t in singles[ci]:
+            assert b.slot(s).get(0) == t.get(0)
+    m.close()
