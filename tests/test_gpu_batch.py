@@ -266,7 +266,7 @@ def test_prepare_then_install_equals_load():
     th.join()
     assert out["rc"] == A.AB_OK and out["cls"] == cls and out["failed"] == 0
     b = A.Batch(cls + (0,), capacity=2, max_steps=8)
-    assert L.ab_batch_ready(b.h) == 1
+    assert L.ab_batch_ready(b.h) == 2                        # idle
     A._check(L.ab_batch_install(b.h, 1, out["p"]))           # takes ownership
     b.Ns[1], b.bases[1] = N, 3                                # what the Python wrapper keeps for get()
     b.load(0, N, 3)
@@ -277,7 +277,7 @@ def test_prepare_then_install_equals_load():
     assert np.array_equal(b.slot(0).read_register(0), b.slot(1).read_register(0))
     assert b.slot(1).get(0) == pow(3, 255, N)
     b.synchronize()
-    assert L.ab_batch_ready(b.h) == 1
+    assert L.ab_batch_ready(b.h) == 2
 
 
 def test_mixed_group_equals_single_transforms():
