@@ -153,6 +153,26 @@ def exponent_bits(N, start, count):
     return int(format(window, "0%db" % count)[::-1], 2)
 
 
+def issue_bound(names, per_ms, dom, instr, sq_us, sms, mhz):
+    """Issue bound of the dominant launch and of the critical path (the R-domain
+    chain, names[3:]): their warp instructions (ncu) at one instruction per clock
+    on each of the 4 schedulers of every SM, at the sampled SM clock; None when
+    a count is missing."""
+    chain = names[3:]
+    if not all(nm in instr for nm in chain + [names[dom]]):
+        return None
+    rate = sms * 4 * mhz * 1e6                           # warp instructions per second
+    ms_of = dict(zip(names, per_ms))
+    n_dom, n_chain = instr[names[dom]], sum(instr[nm] for nm in chain)
+    return {"sms": sms, "sm_mhz": mhz,
+            "dominant": {"kernel": names[dom], "warp_instructions": n_dom, "bound_us": round(n_dom / rate * 1e6, 2),
+                         "us": round(per_ms[dom] * 1e3, 2), "frac": round(n_dom / rate / (per_ms[dom] * 1e-3), 3)},
+            "critical_path": {"launches": chain, "warp_instructions": n_chain, "bound_us": round(n_chain / rate * 1e6, 2),
+                              "us_alone": round(sum(ms_of[nm] for nm in chain) * 1e3, 2),
+                              "frac_of_squaring": round(n_chain / rate / (sq_us * 1e-6), 3)},
+            "source": "warp instructions per launch from profiles/ncu_traffic.json (ncu smsp__inst_executed.sum)"}
+
+
 def run_ours(args, world, rank, local, pg):
     import annie_b200 as A
     from annie_b200.synth import Xoshiro256ss
@@ -235,11 +255,13 @@ def run_ours(args, world, rank, local, pg):
         gbs = u * A_bytes / (ms * 1e-3) / 1e9
         kernels.append({"name": nm, "ms": round(ms, 5), "alg_bytes": u * A_bytes, "GBps": round(gbs, 1)})
     dom = max(range(len(per)), key=lambda i: per[i])
-    traffic = None
+    traffic, instr = None, {}
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(names[dom])
+            tj = json.load(f)
+        traffic = tj.get(names[dom])
+        instr = tj.get("_instructions", {})
     sq_ms = sum(per)
     roof = {
         "bound": "hbm", "kernel": names[dom],
@@ -254,6 +276,12 @@ def run_ours(args, world, rank, local, pg):
                          "serial_launch_sum_ms": round(sq_ms, 5)},
         "kernels": kernels,
     }
+    if instr:
+        import torch
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        issue = issue_bound(names, per, dom, instr, value, sms, (clk or {}).get("sm_mhz") or 1965.0)
+        if issue is not None:
+            roof["issue"] = issue
 
     # ---- parity window (the same window the CPU-baseline leg runs on the
     # reference): Reg0 = 1, Reg1 = Reg0, PARITY_WINDOW iterations of the test

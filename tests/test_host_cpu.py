@@ -87,3 +87,16 @@ def test_periodic_gerbicz_li_check_detects_and_rolls_back(monkeypatch):
     res = bench.run_proth2m_workload(args)
     assert res["gl_check"]["passed"]
     assert res["injected_error"]["detected"] and res["injected_error"]["rolled_back_and_verified"]
+
+
+def test_issue_bound_of_the_bench_line():
+    # the bench's issue bound: warp instructions / (SMs x 4 schedulers x clock)
+    names = ["a", "b", "c", "r0", "r1", "r2", "r3", "r4", "r5"]
+    per = [0.01, 0.02, 0.02, 0.03, 0.03, 0.03, 0.03, 0.03, 0.04]
+    instr = {nm: 1_000_000 for nm in names[3:]}
+    out = bench.issue_bound(names, per, 8, instr, 200.0, 100, 1000.0)
+    rate = 100 * 4 * 1000.0e6
+    assert out["dominant"]["bound_us"] == round(1e6 / rate * 1e6, 2)
+    assert out["critical_path"]["warp_instructions"] == 6_000_000
+    assert out["critical_path"]["frac_of_squaring"] == round(6e6 / rate / 200e-6, 3)
+    assert bench.issue_bound(names, per, 8, {"r0": 1}, 200.0, 100, 1000.0) is None
