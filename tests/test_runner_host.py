@@ -85,3 +85,16 @@ def test_runner_decides_without_a_transform():
         assert r.stats()["batches"] == 0                 # no batch was created
     finally:
         r.close()
+
+
+def test_runner_rejects_bad_epoch_options():
+    _lib()
+    with pytest.raises(A.EngineError):
+        A.Runner(latency_ln=-1)
+    with pytest.raises(A.EngineError):
+        A.Runner(latency_ln=12, epoch_us=0)
+    r = A.Runner(latency_ln=12, epoch_us=5000)          # host only until a test needs a transform
+    r.submit(1000003, tag=7)
+    res = _drain(r, 1)
+    assert res[7]["decided_early"] == 1
+    r.close()
