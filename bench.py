@@ -823,6 +823,31 @@ def proth2m_parity(args, count=64):
     return rec
 
 
+def side_c1():
+    """C1 as a sub-object of the default line: the full Fermat test (base 3,
+    Gerbicz-Li block 256) of the 262,144-bit seeded N, timed end to end through
+    ab_prp_check, with its RES64 against the reference's (the golden fixture
+    that tests/golden/make_golden.py took from the reference's transformCPU)."""
+    import annie_b200 as A
+    from annie_b200.synth import Xoshiro256ss
+    rng = Xoshiro256ss(4)
+    while True:
+        N = rng.random_odd(262144)
+        if all(N % p for p in SMALL_PRIMES):
+            break
+    with open(os.path.join(ROOT, "tests", "golden", "prp_vectors.json")) as f:
+        gold = [v for v in json.load(f) if v["form"] == "random_odd" and v["bits"] == 262144 and v["seed"] == 4][0]
+    A.prp_check(N, base=3)                                 # warm-up (graphs, twiddles)
+    t0 = time.perf_counter()
+    res = A.prp_check(N, base=3)
+    sec = time.perf_counter() - t0
+    return {"bits": 262144, "seconds": round(sec, 3), "squarings": res["squarings"],
+            "us_per_squaring_e2e": round(sec * 1e6 / res["squarings"], 2), "params": [res["K"], res["pck"], res["ln"], res["lbase"]],
+            "res64": "%016X" % res["res64"], "res64_equals_reference": "%016X" % res["res64"] == gold["res64"],
+            "gl_validated": res["status"] == 0,
+            "workload": "Fermat PRP base 3 on the seeded random odd 262,144-bit N (xoshiro256** seed 4, no factor below 2000), full test"}
+
+
 def side_batch(args):
     """C4 as a sub-object of the default line (a shorter runner window)."""
     import copy
@@ -914,8 +939,10 @@ def main():
                       % (res["cores"], PARITY_WINDOW, res["single_us"])}
     line["parity"] = parity_record(regs, res)
     if world == 1 and not args.no_side_workloads:
-        # the other configurations the driver should see measured: the Proth
-        # n = 2,000,000 test (C2) and the 4096-candidate batch (C4)
+        # the other configurations the driver should see measured: the full
+        # 262,144-bit test (C1), the Proth n = 2,000,000 test (C2), the
+        # 4096-candidate batch (C4) and the serving window (C5)
+        line["c1"] = side_c1()
         line["proth2M"] = side_proth2m(args)
         line["batch"] = side_batch(args)
         lo, hi = args.serve_bits
