@@ -409,7 +409,15 @@ struct ab_runner
 			--outstanding;
 			ab_prepared * pp = j->prep;
 			j->prep = nullptr;
-			ck(ab_batch_install(c->b, slot, pp));
+			if (ab_batch_install(c->b, slot, pp) != AB_OK)
+			{
+				// the test ends with the error; the ones still waiting stay queued
+				const std::string m = std::string("the test could not be set up on the device: ") + ab_last_error();
+				finish(j, -1, m.c_str());
+				for (Job * w : prepared) later.push_back(w);
+				prepared.swap(later);
+				throw rt_error(m);
+			}
 			c->slots[slot] = j;
 			ab_transform * v = ab_batch_slot(c->b, slot);
 			ck(ab_set1(v));
