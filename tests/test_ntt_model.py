@@ -40,3 +40,22 @@ def test_model_products_are_exact(K, bits, ln):
             wrap = 1 << (32 * K)
             exp = [((e + wrap // 2) % wrap) - wrap // 2 for e in exp]
             assert got == exp, "K=%d ln=%d %s %s" % (K, ln, "Q" if q else "R", "square" if yy is None else "mul")
+
+
+def test_row_twiddles_factor_into_row_constant_and_shared_table():
+    # the twiddle of row r (of HR = 2^a rows) at row level t and index m is
+    # w[(HR + r) 2^t] * beta_t[m], beta_t the row-independent domain-R table of
+    # the level with 2^t polynomials (positions 2^t + m of a longer transform):
+    # the structure a twisted row transform with one shared table relies on
+    ln, a = 17, 5
+    HR = 1 << a
+    for k in (0, 5):
+        p = M.TPRIMES[k]
+        beta = M.tables(14, k, False)[0].astype(object)
+        for q in (False, True):
+            w = M.tables(ln, k, q)[0].astype(object)
+            for r in (0, 3, HR - 1):
+                for t in range(ln - 1 - a):
+                    base = (HR + r) << t
+                    for m in range(0, 1 << t, max(1, (1 << t) // 5)):
+                        assert w[base + m] == w[base] * beta[(1 << t) + m] % p
