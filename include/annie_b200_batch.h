@@ -84,7 +84,8 @@ int ab_batch_launch_count(const ab_batch * b, uint64_t * count);
    from a device table; the slots' results are those of ab_batch_steps on
    each batch.  While in a group, a batch is stepped through the group only
    (its slots stay usable with every ab_transform call, and
-   ab_batch_set_geometry makes the group re-record). */
+   ab_batch_set_geometry makes the group re-record); destroy the group before
+   its batches. */
 typedef struct ab_mixed ab_mixed;
 int ab_mixed_create(ab_batch * const * batches, int count, int max_steps, ab_mixed ** out);
 void ab_mixed_destroy(ab_mixed * m);
